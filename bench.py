@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark of the two-surface boundary-integral solve on B200.
+
+Workload (one "step"): the two-surface problem of highreg_stokes_2surf at
+h = 1/64 (27,934 + 29,084 quadrature points, n = 171,054 unknowns), KITC
+treecode P = 6, N0 = 2000, theta = 0.6: the right-hand side b = -2/3 S[f]
+(four Stokeslet sums) and the GMRES solve of (I - 2/3 D) u = b to a 1e-10
+relative residual (restart 50), all on the device, FP64.
+
+value: pair interactions per second of the whole step (regularized and plain
+target-source pairs plus target-proxy pairs), summed over ranks and divided
+by the slowest rank's time. Each timed step is preceded by an L2 flush
+(a 256 MB device write) outside its CUDA-event pair.
+
+--impl reference times the reference's own CPU implementation (the
+unmodified highreg_stokes_2surf compiled into oracle/_ref) on the host cores:
+each step is one reference operator application solve_IE_1step at the same
+geometry and treecode parameters; its pairs/s uses the same pair count.
+
+Multi-GPU: the path does not shard (one B200 per problem); --gpus N runs N
+independent replicas, one per rank, with no data-path collective.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "high-order-regularization_b200"))
+
+H_INV = 64
+P, N0, THETA = 6, 2000, 0.6
+RESTART, TOL = 50, 1e-10
+
+
+def dist_info():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
+            self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % self.device)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def max_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(v, world):
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def pairs_of(work):
+    return work["direct_pairs_near"] + work["direct_pairs_far"] + work["proxy_pairs"]
+
+
+def cpu_reference_matvec(geo_pairs, seconds_budget=None):
+    """One reference operator application on the host cores (oracle/_ref)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    from oracle import Ref2S
+
+    R = Ref2S(P, N0).setup(H_INV)
+    u = np.random.default_rng(0).standard_normal(3 * sum(R.nq))
+    t0 = time.perf_counter()
+    R.matvec(u)
+    dt = time.perf_counter() - t0
+    return R, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import highreg
+    from oracle import Ref2S, ref_available
+
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    line = {"impl": "reference", "metric": "2-surf solve time to 1e-10 residual (plain FP64 vs mixed+warm-start); pairs/s",
+            "unit": "pairs/s", "higher_is_better": True, "n_gpus": args.gpus}
+    if not ref_available():
+        line["unavailable"] = "reference build (oracle/_ref) not present on this machine"
+        print(json.dumps(line))
+        return
+    # pair count of one operator application: same tree decisions as ours
+    geo = highreg.Geometry2S(H_INV).scene
+    n_pairs = None
+    try:
+        ctx = highreg.Context(0)
+        plan = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=P, N0=N0, theta=THETA)
+        n_pairs = pairs_of(plan.work(0))
+        plan.close()
+        ctx.close()
+    except Exception:
+        pass
+    R = Ref2S(P, N0).setup(H_INV)
+    u = np.random.default_rng(0).standard_normal(3 * sum(R.nq))
+    for _ in range(args.warmup):
+        R.matvec(u)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        R.matvec(u)
+        times.append(time.perf_counter() - t0)
+    t = sum(times)
+    value = n_pairs * args.steps / t if n_pairs else None
+    line.update({"value": value, "steps": args.steps, "warmup": args.warmup,
+                 "ms_per_step": 1e3 * t / args.steps, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                 "data": "synthetic (reference geometry generated in-process)",
+                 "config": {"workload": "two-surface operator application solve_IE_1step, h=1/64, KITC P=6 N0=2000 theta=0.6",
+                            "pairs_per_step": n_pairs},
+                 "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                                  "kind": "reference",
+                                  "sample": "%d reference matvecs (solve_IE_1step) at h=1/64" % args.steps},
+                 "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import highreg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    geo = highreg.Geometry2S(H_INV).scene
+    ctx = highreg.Context(local_rank)
+    plan = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=P, N0=N0, theta=THETA)
+    n = plan.n
+    f1 = torch.tensor(geo["f0"], dtype=torch.float64, device=dev)
+    f2 = torch.tensor(geo["f1"], dtype=torch.float64, device=dev)
+    b = torch.zeros(n, dtype=torch.float64, device=dev)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    w_rhs = plan.work(1)
+    w_mv = plan.work(0)
+    stream = torch.cuda.ExternalStream(plan.stream(), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()
+
+    def step():
+        plan.rhs_dev(f1, f2, b)
+        return plan.solve_dev(b, x, restart=RESTART, tol=TOL, precision=highreg.HR_FP64)
+
+    for _ in range(max(3, args.warmup)):
+        rep = step()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = ClockSampler(local_rank)
+    clk.start()
+    l0 = ctx.launches
+    times, reps = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rep = step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        reps.append(rep)
+    torch.cuda.synchronize()
+    launches = ctx.launches - l0
+    clocks = clk.stop()
+    barrier(world)
+    t_local = sum(times) / 1e3
+    it = reps[-1]["iterations"]
+    mv_per_step = reps[-1]["matvecs_fp64"] + reps[-1]["matvecs_mixed"]
+    pairs_step = pairs_of(w_rhs) + mv_per_step * pairs_of(w_mv)
+    t_max = max_over_ranks(t_local, world)
+    pairs_total = sum_over_ranks(pairs_step * args.steps, world)
+    value = pairs_total / t_max
+
+    # dominant kernel: the stresslet batch of the operator (one launch per matvec)
+    plan.matvec_dev(x, b)
+    ms_dl = plan.time_batch(0, 20)
+    moment_flops = 2.0 * 12 * w_mv["moment_terms"]
+    fl_launch = w_mv["flops"] - moment_flops
+    peak = ctx.fp64_peak()
+    achieved = fl_launch / (ms_dl * 1e-3)
+    roofline = {"bound": "fp64", "kernel": "eval_kernel<F_DL> (stresslet batch, one launch per matvec)",
+                "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": None,
+                "flops_per_launch": fl_launch, "ms_per_launch": ms_dl,
+                "peak_source": "measured FP64 FMA loop (hr_measure_fp64_peak) on this GPU"}
+
+    # end to end through the C ABI with host buffers: scene upload + plan
+    # (trees, interaction lists, stencils) + RHS + solve + solution read back
+    e2e_times = []
+    h2d = sum(np.asarray(v).nbytes for k, v in geo.items() if isinstance(v, np.ndarray))
+    for _ in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p2 = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=P, N0=N0, theta=THETA)
+        bh = p2.rhs(geo["f0"], geo["f1"])
+        xh, r2 = p2.solve(bh, restart=RESTART, tol=TOL)
+        e2e_times.append(time.perf_counter() - t0)
+        p2.close()
+    e2e_t = max_over_ranks(statistics.median(e2e_times), world)
+    e2e = {"value": sum_over_ranks(pairs_step, world) / e2e_t, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(8 * n), "seconds_per_step": e2e_t}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+                _, dt = cpu_reference_matvec(None)
+                cpu = {"value": pairs_of(w_mv) / dt, "unit": "pairs/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                       "kind": "reference",
+                       "sample": "one reference operator application (solve_IE_1step, h=1/64, P=6, N0=2000), %.1f s" % dt}
+            except Exception as e:  # reference build absent
+                cpu = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
+                       "sample": "unavailable: %s" % e}
+        line = {"metric": "2-surf solve time to 1e-10 residual (plain FP64 vs mixed+warm-start); pairs/s",
+                "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (the reference's two-spheroid geometry generated in-process)",
+                "config": {"workload": "two-surface solve h=1/64 (n=%d), KITC P=6 N0=2000 theta=0.6, GMRES restart 50 tol 1e-10, plain FP64" % n,
+                           "global_batch": world, "parallelism": "replicas" if world > 1 else "single",
+                           "l2": "flushed (256 MB write) before each timed step",
+                           "gmres_iterations": it, "matvecs_per_step": mv_per_step,
+                           "pairs_per_step": pairs_step, "solve_seconds": t_max / args.steps,
+                           "final_residual": reps[-1]["residual"]},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+                "gpu_launches": launches}
+        print(json.dumps(line))
+    plan.close()
+    ctx.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local_rank = dist_info()
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

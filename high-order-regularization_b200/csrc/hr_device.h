@@ -1,0 +1,96 @@
+// hr_device.h — device task descriptors and kernel launchers (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "hr_engine.h"
+
+namespace hr {
+
+// One boundary sum: a source surface (tree order SoA) evaluated at a target
+// set (reference order). All pointers are device pointers.
+struct EvalTask {
+  int kind;       // Kind
+  int jump_mode;  // DL kinds: 0 = treecode convention, 1 = direct-sum convention
+  int P1, Pf;     // treecode degree + 1 and (P+1)^3
+  int C;          // moment channels stored per node (6 SL, 12 DL)
+  int nt;         // number of targets
+  int mixed;      // 1: far pairs / proxies in FP32 with FP64 accumulation
+  int pad;
+  double DEL;     // regularization length delta
+  double scale;   // final factor of the sum (1/8pi, -6/8pi, ...)
+  const double *sx, *sy, *sz, *snx, *sny, *snz, *sa;  // sources, tree order
+  const double *qx, *qy, *qz;                         // density, tree order
+  const int *node_m0, *node_m1;                       // inclusive member ranges
+  const double* tcheb;                                // 3*P1 per node
+  const double* mom;                                  // C*Pf per node
+  const int* tord;                                    // target order -> target index
+  const double* txyz;                                 // 3nt targets
+  const double* tb;                                   // nt signed distances
+  const uint8_t* tnear;                               // nt regularized-branch flag
+  const double* tf0;                                  // 3nt nearest force (SL off, E2G)
+  const double *tx0, *tn0, *tg0;                      // 3nt nearest point, normal, density
+  const double *tq, *tnrm;                            // 3nt own density and normal (on-surface)
+  double* out;                                        // 3nt (or nt for pressure)
+  const Entry* entries;                               // interaction entries
+  const int* blk_start;                               // per target block, into entries
+  unsigned long long* counters;  // [0] regularized pairs [1] near-target plain [2] far-target [3] proxy
+};
+
+struct BlockRef {
+  int task;
+  int blk;
+};
+
+enum Family : int { F_SL = 0, F_DL = 1, F_E2G = 2 };
+
+// Evaluates every block of a combined block list in one launch.
+void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_blocks, int nblocks,
+                 cudaStream_t st);
+
+// Upward pass: proxy moments of every non-root node of a tree.
+struct MomItem {
+  int node;
+  int s0;  // first source (tree order)
+  int s1;  // one past last source
+  int out; // partial slot
+};
+void launch_moments(int dl, const MomItem* d_items, int nitems, int P1, const double* tcheb,
+                    const double* x, const double* y, const double* z, const double* nx,
+                    const double* ny, const double* nz, const double* a, const double* qx,
+                    const double* qy, const double* qz, double* partial, cudaStream_t st);
+void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_start,
+                           const double* partial, double* mom, cudaStream_t st);
+
+// Gathers interleaved reference-order density into tree-order SoA.
+void launch_permute(int n, const int* perm, const double* q3, double* qx, double* qy, double* qz,
+                    cudaStream_t st);
+void launch_permute_soa(int n, const int* perm, const double* src, double* dst, cudaStream_t st);
+
+// Six-point density interpolation at nearest points.
+void launch_interp(int ne, const int* tgt, const int* idx, const double* pq, const double* g,
+                   double* g0, cudaStream_t st);
+
+// Two-surface combine steps.
+void launch_matvec_combine(int n, double factor, const double* x, const double* on,
+                           const double* comp, double* y, cudaStream_t st);
+void launch_rhs_combine(int n, double factor, const double* on, const double* comp, double* b,
+                        cudaStream_t st);
+
+// Vector kernels for GMRES (deterministic reductions).
+constexpr int kRedBlocks = 296;
+void launch_dots(int n, int ncols, const double* V, long ldv, const double* w, double* partial,
+                 cudaStream_t st);
+void launch_dots_finalize(int ncols, const double* partial, double* out, cudaStream_t st);
+void launch_axpy_multi(int n, int ncols, const double* V, long ldv, const double* coef,
+                       double sign, double* w, cudaStream_t st);
+void launch_scale(int n, const double* s_dev, double* w, cudaStream_t st);
+void launch_scale_host(int n, double s, double* w, cudaStream_t st);
+void launch_sub(int n, const double* a, const double* b, double* out, cudaStream_t st);
+void launch_copy(int n, const double* a, double* out, cudaStream_t st);
+
+// FP64 FMA peak loop.
+void launch_fma_peak(double* out, int iters, int blocks, cudaStream_t st);
+
+}  // namespace hr

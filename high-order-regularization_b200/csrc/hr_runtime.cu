@@ -1,0 +1,166 @@
+// hr_runtime.cu — device trees, target lists, stencils and evaluation batches.
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "hr_runtime.h"
+
+namespace hr {
+
+void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direct,
+                    cudaStream_t st) {
+  HR_REQUIRE(S.n >= 0 && (S.n == 0 || (S.xyz && S.nrml && S.area)), "surface arrays missing");
+  HR_REQUIRE(P >= 1 && P + 1 <= 16, "treecode degree P must be in [1, 15]");
+  HR_REQUIRE(N0 >= 1, "leaf size N0 must be >= 1");
+  host = build_tree(S.n, S.xyz, S.center, P, N0, theta, direct);
+  n = S.n;
+  nn = host.nnodes();
+  P1 = P + 1;
+  Pf = P1 * P1 * P1;
+  std::vector<double> hx(n), hy(n), hz(n), hnx(n), hny(n), hnz(n), ha(n);
+  for (int p = 0; p < n; p++) {
+    int o = host.perm[p];
+    hx[p] = S.xyz[3 * o];
+    hy[p] = S.xyz[3 * o + 1];
+    hz[p] = S.xyz[3 * o + 2];
+    hnx[p] = S.nrml[3 * o];
+    hny[p] = S.nrml[3 * o + 1];
+    hnz[p] = S.nrml[3 * o + 2];
+    ha[p] = S.area[o];
+  }
+  x.upload(hx, st);
+  y.upload(hy, st);
+  z.upload(hz, st);
+  nx.upload(hnx, st);
+  ny.upload(hny, st);
+  nz.upload(hnz, st);
+  a.upload(ha, st);
+  perm.upload(host.perm, st);
+  m0.upload(host.m0, st);
+  m1.upload(host.m1, st);
+  tcheb.upload(host.tcheb, st);
+  qx.alloc(n);
+  qy.alloc(n);
+  qz.alloc(n);
+  // upward-pass items: every non-root node (the root's moments stay zero, as
+  // in the reference, which skips it: 2S/KITC.cpp:1446), in chunks of sources.
+  std::vector<MomItem> it;
+  std::vector<int> start(nn + 1, 0);
+  const int chunk = 512;
+  moment_terms = 0;
+  for (int c = 0; c < nn; c++) {
+    start[c] = (int)it.size();
+    if (c == 0 || direct) continue;
+    for (int s = host.m0[c]; s <= host.m1[c]; s += chunk) {
+      MomItem m;
+      m.node = c;
+      m.s0 = s;
+      m.s1 = std::min(host.m1[c] + 1, s + chunk);
+      m.out = (int)it.size();
+      it.push_back(m);
+    }
+    moment_terms += (long long)Pf * (host.m1[c] - host.m0[c] + 1);
+  }
+  start[nn] = (int)it.size();
+  nitems = (int)it.size();
+  items.upload(it, st);
+  item_start.upload(start, st);
+  partial.alloc((size_t)std::max(1, nitems) * 12 * Pf);
+  mom.alloc((size_t)nn * 12 * Pf);
+  mom.zero(st);
+}
+
+void DevTree::set_density(Ctx& C, const double* q3_dev, bool dl, bool moments) {
+  launch_permute(n, perm.p, q3_dev, qx.p, qy.p, qz.p, C.stream);
+  C.launches++;
+  if (moments && nitems > 0) {
+    launch_moments(dl ? 1 : 0, items.p, nitems, P1, tcheb.p, x.p, y.p, z.p, nx.p, ny.p, nz.p, a.p,
+                   qx.p, qy.p, qz.p, partial.p, C.stream);
+    launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, C.stream);
+    C.launches += 2;
+  }
+}
+
+void DevLists::build(const Tree& T, int nt, const double* txyz, const uint8_t* near,
+                     cudaStream_t st) {
+  host = build_lists(T, nt, txyz, near);
+  tord.upload(host.tord, st);
+  blk_start.upload(host.blk_start, st);
+  entries.upload(host.entries, st);
+}
+
+void DevStencils::build(const Stencils& S, cudaStream_t st) {
+  ne = (int)S.tgt.size();
+  tgt.upload(S.tgt, st);
+  idx.upload(S.idx, st);
+  pq.upload(S.pq, st);
+}
+
+EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const DevLists& L,
+                   const DevTargets& tg, double* out) {
+  EvalTask k;
+  memset(&k, 0, sizeof(k));
+  k.kind = kind;
+  k.jump_mode = 0;
+  k.P1 = T.P1;
+  k.Pf = T.Pf;
+  k.C = (kind == K_DL_ON || kind == K_DL_OFF) ? 12 : 6;
+  k.nt = tg.n;
+  k.mixed = 0;
+  k.DEL = DEL;
+  k.scale = scale;
+  k.sx = T.x.p;
+  k.sy = T.y.p;
+  k.sz = T.z.p;
+  k.snx = T.nx.p;
+  k.sny = T.ny.p;
+  k.snz = T.nz.p;
+  k.sa = T.a.p;
+  k.qx = T.qx.p;
+  k.qy = T.qy.p;
+  k.qz = T.qz.p;
+  k.node_m0 = T.m0.p;
+  k.node_m1 = T.m1.p;
+  k.tcheb = T.tcheb.p;
+  k.mom = T.mom.p;
+  k.tord = L.tord.p;
+  k.txyz = tg.xyz.p;
+  k.tb = tg.b.p;
+  k.tnear = tg.near.p;
+  k.tf0 = tg.f0.p;
+  k.tx0 = tg.x0.p;
+  k.tn0 = tg.n0.p;
+  k.tg0 = tg.g0.p;
+  k.tq = nullptr;
+  k.tnrm = tg.nrm.p;
+  k.out = out;
+  k.entries = L.entries.p;
+  k.blk_start = L.blk_start.p;
+  k.counters = nullptr;
+  return k;
+}
+
+void Batch::finalize(cudaStream_t st) {
+  std::vector<std::pair<double, BlockRef>> all;
+  for (size_t t = 0; t < tasks.size(); t++) {
+    const Lists& L = *lists[t];
+    for (int b = 0; b < L.nblocks(); b++) all.push_back({L.blk_cost[b], BlockRef{(int)t, b}});
+  }
+  // longest first: the hardware dispatches CTAs roughly in index order
+  std::stable_sort(all.begin(), all.end(),
+                   [](const std::pair<double, BlockRef>& a, const std::pair<double, BlockRef>& b) {
+                     return a.first > b.first;
+                   });
+  std::vector<BlockRef> br(all.size());
+  for (size_t i = 0; i < all.size(); i++) br[i] = all[i].second;
+  nblocks = (int)br.size();
+  d_blocks.upload(br, st);
+  d_tasks.upload(tasks, st);
+}
+
+void Batch::launch(Ctx& C) {
+  launch_eval(family, d_tasks.p, d_blocks.p, nblocks, C.stream);
+  C.launches++;
+}
+
+}  // namespace hr

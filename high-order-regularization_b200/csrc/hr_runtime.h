@@ -1,0 +1,142 @@
+// hr_runtime.h — context, device buffers and the device-resident objects the
+// C ABI is built from (internal).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/highreg_b200.h"
+#include "hr_device.h"
+#include "hr_engine.h"
+
+namespace hr {
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define HR_CHECK_CUDA(call)                                                                  \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw ::hr::Error(HR_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));    \
+  } while (0)
+
+#define HR_REQUIRE(cond, msg)                                   \
+  do {                                                          \
+    if (!(cond)) throw ::hr::Error(HR_ERR_ARG, std::string(msg)); \
+  } while (0)
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    if (count == 0) count = 1;
+    HR_CHECK_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    n = count;
+  }
+  void upload(const T* h, size_t count, cudaStream_t st) {
+    alloc(count);
+    if (h && count) HR_CHECK_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, st));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t st) { upload(v.data(), v.size(), st); }
+  void zero(cudaStream_t st) {
+    if (p) HR_CHECK_CUDA(cudaMemsetAsync(p, 0, n * sizeof(T), st));
+  }
+};
+
+struct Ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  long long launches = 0;
+  DBuf<unsigned long long> counters;  // [0] reg pairs [1] plain pairs [2] proxies
+};
+
+// A surface on the device: sources in tree order, its tree, density buffers
+// and the upward-pass work items.
+struct DevTree {
+  Tree host;
+  int n = 0, nn = 0, P1 = 0, Pf = 0;
+  DBuf<double> x, y, z, nx, ny, nz, a;
+  DBuf<int> perm, m0, m1;
+  DBuf<double> tcheb;
+  DBuf<double> qx, qy, qz;
+  DBuf<double> mom;  // nn * 12 * Pf
+  DBuf<MomItem> items;
+  DBuf<int> item_start;
+  DBuf<double> partial;
+  int nitems = 0;
+  long long moment_terms = 0;  // sum over non-root nodes of Pf * members
+  void build(const hr_surface& S, int P, int N0, double theta, bool direct, cudaStream_t st);
+  // density (reference order, interleaved, device) -> tree-order SoA (+ moments)
+  void set_density(Ctx& C, const double* q3_dev, bool dl, bool moments);
+};
+
+// Target data on the device, reference order.
+struct DevTargets {
+  int n = 0;
+  DBuf<double> xyz, b, x0, n0, f0, g0;
+  DBuf<uint8_t> near;
+  DBuf<double> nrm;  // own normals for on-surface targets
+};
+
+struct DevLists {
+  Lists host;
+  DBuf<int> tord, blk_start;
+  DBuf<Entry> entries;
+  void build(const Tree& T, int nt, const double* txyz, const uint8_t* near, cudaStream_t st);
+};
+
+struct DevStencils {
+  int ne = 0;
+  DBuf<int> tgt, idx;
+  DBuf<double> pq;
+  void build(const Stencils& S, cudaStream_t st);
+};
+
+// A batch of boundary sums evaluated in one launch.
+struct Batch {
+  int family = F_SL;
+  std::vector<EvalTask> tasks;
+  std::vector<const Lists*> lists;
+  DBuf<EvalTask> d_tasks;
+  DBuf<BlockRef> d_blocks;
+  int nblocks = 0;
+  void finalize(cudaStream_t st);  // builds the combined cost-sorted block list
+  void launch(Ctx& C);
+};
+
+EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const DevLists& L,
+                   const DevTargets& tg, double* out);
+
+}  // namespace hr

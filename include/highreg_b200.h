@@ -1,0 +1,234 @@
+/*
+ * highreg_b200.h — C ABI of the B200 (sm_100a) implementation of the
+ * regularized Stokeslet / stresslet boundary sums of Beale & Tlupova's
+ * high-order regularization (reference: stlupova/high-order-regularization).
+ *
+ * Plain pointers and sizes only. Unless an entry point says otherwise,
+ * pointers are HOST pointers, arrays of points / vector fields are
+ * interleaved xyz (v[3*j+k], as the reference's f[3*j+k]), results are
+ * written into caller-owned buffers, and every call is synchronous at return.
+ * Every function returns HR_OK (0) or a nonzero status; hr_last_error() gives
+ * the message. A context is not thread-safe; use one context per thread.
+ *
+ * Reference citations are file:line within the reference project
+ * (2S = highreg_stokes_2surf, E2G = highreg_stokes_extend_to_grid).
+ */
+#ifndef HIGHREG_B200_H
+#define HIGHREG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HR_OK 0
+#define HR_ERR_ARG 1           /* bad argument (size, null pointer, unsupported option) */
+#define HR_ERR_CUDA 2          /* CUDA / cuFFT runtime failure */
+#define HR_ERR_NAN 3           /* non-finite value detected in an input or output */
+#define HR_ERR_NOT_CONVERGED 4 /* GMRES hit its iteration cap or stagnated */
+#define HR_ERR_NO_DEVICE 5     /* no usable sm_100 device */
+#define HR_ERR_STATE 6         /* object used in the wrong state */
+
+/* evaluation mode and precision */
+#define HR_DIRECT 0 /* all-pairs sums: eval_Stokes_*_{on,off}Surf (2S/stokeslets.cpp, 2S/stresslets.cpp) */
+#define HR_TREE 1   /* KITC treecode: eval_Stokes_*_tree (2S/KITC.cpp:1389-1830) */
+#define HR_FP64 0   /* all pairs in FP64 */
+#define HR_MIXED 1  /* far pairs / proxy interactions in FP32 with FP64 per-target accumulation */
+
+typedef struct hr_ctx hr_ctx;
+
+/* A quadrature surface: grid-line-intersection points with partition-of-unity
+ * area weights (the reference's vector<Surf_point>, 2S/utilities.h:30-39),
+ * as host SoA arrays in the reference's order. */
+typedef struct {
+  int n;
+  const double* xyz;    /* 3n points */
+  const double* nrml;   /* 3n unit normals */
+  const double* area;   /* n area elements h^2 sigma_i(n)/|n_i| */
+  const int* plane;     /* n grid-line family of each point (0,1,2), may be NULL */
+  double center[3];     /* surface centre: the treecode root box is centre + [-1,1]^3 */
+} hr_surface;
+
+/* Target points with their nearest-surface data (the reference's
+ * vector<Target_point>, 2S/utilities.h:41-53). For on-surface sums the
+ * targets are the surface's own points and only xyz is read. */
+typedef struct {
+  int n;
+  const double* xyz;  /* 3n target points */
+  const double* b;    /* n signed distance to the source surface */
+  const double* x0;   /* 3n nearest surface point */
+  const double* n0;   /* 3n unit normal at x0 */
+  const int* nrst;    /* n reference flag: 0 = no subtraction / no interpolation
+                         (|b|/delta > 8), else the nearest quadrature index */
+  const int* i123;    /* 3n Monge-patch indices (ind1, ind2, ind3) of each target */
+} hr_targets;
+
+typedef struct {
+  int mode;      /* HR_DIRECT or HR_TREE */
+  int P;         /* treecode interpolation degree (2S/KITC.h:14) */
+  int N0;        /* treecode leaf size (2S/KITC.h:16) */
+  double theta;  /* treecode MAC parameter, sq_theta = theta^2 (2S/KITC.h:17) */
+  int precision; /* HR_FP64 or HR_MIXED */
+} hr_eval_opts;
+
+/* ---------------------------------------------------------------- context */
+int hr_ctx_create(int device, hr_ctx** out);
+void hr_ctx_destroy(hr_ctx* ctx);
+const char* hr_last_error(const hr_ctx* ctx);
+/* number of kernel launches issued by this context so far */
+long long hr_ctx_launch_count(const hr_ctx* ctx);
+
+/* ------------------------------------------------- boundary sums (drop-in) */
+/* eval_Stokes_SL_onSurf[_tree]: 2S/stokeslets.cpp:141-180, 2S/KITC.cpp:1389-1492.
+ * f: 3n density on S; out: 3n Stokeslet sum at S's own points. */
+int hr_stokes_sl_onsurf(hr_ctx* ctx, const hr_eval_opts* opt, double delta, const hr_surface* S,
+                        const double* f, double* out);
+/* eval_Stokes_SL_offSurf[_tree]: 2S/stokeslets.cpp:12-86, 2S/KITC.cpp:1496-1602.
+ * f0: 3nt force at each target's nearest point (Target_point::nrst_f). */
+int hr_stokes_sl_offsurf(hr_ctx* ctx, const hr_eval_opts* opt, double delta, const hr_surface* S,
+                         const double* f, const hr_targets* T, const double* f0, double* out);
+/* eval_Stokes_DL_onSurf[_tree]: 2S/stresslets.cpp:186-228, 2S/KITC.cpp:1606-1709. */
+int hr_stokes_dl_onsurf(hr_ctx* ctx, const hr_eval_opts* opt, double delta, const hr_surface* S,
+                        const double* g, double* out);
+/* eval_Stokes_DL_offSurf[_tree]: 2S/stresslets.cpp:13-96, 2S/KITC.cpp:1712-1830.
+ * g0: 3nt density at the nearest points (Target_point::nrst_g). The jump term
+ * follows the mode's reference: tree adds g0/2 on the surface and g0 inside,
+ * direct adds g0 inside or when |b| < 1e-14. */
+int hr_stokes_dl_offsurf(hr_ctx* ctx, const hr_eval_opts* opt, double delta, const hr_surface* S,
+                         const double* g, const hr_targets* T, const double* g0, double* out);
+
+/* interpolate_DL_density: 2S/main.cpp:916-1046. Six-point tensor Lagrange
+ * interpolation of g at each target's nearest point x0, on the grid lines of
+ * the Monge plane (i123) of the source surface with spacing h.
+ * S->center is the source surface centre; S->plane is required. */
+int hr_interpolate_dl_density(hr_ctx* ctx, double h, const hr_surface* S, const double* g,
+                              const hr_targets* T, double* g0);
+
+/* ------------------------------------------------ extend-to-grid (E2G) sums */
+/* stokes_SL_away: E2G/stokes.cpp:13-45 (plain Stokeslet, nt targets xyz). */
+int hr_e2g_stokeslet_away(hr_ctx* ctx, const hr_surface* S, const double* f, int nt,
+                          const double* xyz, double* out3);
+/* stokes_pressure_away: E2G/stokes.cpp:102-126. */
+int hr_e2g_pressure_away(hr_ctx* ctx, const hr_surface* S, const double* f, int nt,
+                         const double* xyz, double* out1);
+/* stokes_SL_7ord at band targets: E2G/stokes.cpp:53-97 with f0 = the exact
+ * density at x0 (E2G/main.cpp:1330-1345). f0: 3nt. */
+int hr_e2g_stokeslet_7ord(hr_ctx* ctx, double delta, const hr_surface* S, const double* f,
+                          const hr_targets* T, const double* f0, double* out3);
+/* stokes_pressure_7ord: E2G/stokes.cpp:134-203. */
+int hr_e2g_pressure_7ord(hr_ctx* ctx, double delta, const hr_surface* S, const double* f,
+                         const hr_targets* T, const double* f0, double* out1);
+
+/* fftw_DST_Poisson3d_FD: E2G/main.cpp:1423-1489. In place on a row-major
+ * n^3 host array: DST-I, divide by the eigenvalues of the 4th-order compact
+ * Laplacian, DST-I, scale 1/(2(n+1))^3. */
+int hr_dst_poisson3d(hr_ctx* ctx, int n, double* f);
+
+/* solve_Poisson: E2G/main.cpp:969-1044. Grids are row-major (N+1)^3.
+ * band2: 1 at BAND2 points; outside: 1 at exterior points outside BAND2
+ * (phi > 0 and not in BAND2). u is in/out; p is read when variable = 1..3. */
+int hr_e2g_solve_poisson(hr_ctx* ctx, int N, double L, const uint8_t* band2,
+                         const uint8_t* outside, const double* p, double* u, int variable);
+
+/* --------------------------------------------------- two-surface problem */
+/* The two-surface boundary integral equation (I - 2/3 D) u = b
+ * (2S/main.cpp:140-417). Target set s is the quadrature points of surface s
+ * with nearest data relative to the OTHER surface. */
+typedef struct {
+  hr_surface surf[2];
+  hr_targets tgt[2];
+  const double* f0[2]; /* 3n force at each target's nearest point (for the RHS) */
+  double h;            /* grid spacing */
+  double delta;        /* regularization length */
+} hr_scene2s;
+
+typedef struct {
+  int restart;         /* GMRES restart length (reference: 15, 2S/main.cpp:213) */
+  int max_iter;        /* iteration cap (reference: 100) */
+  double tol;          /* relative residual tolerance (reference: 1e-10) */
+  int precision;       /* HR_FP64, or HR_MIXED: relaxed-precision matvecs */
+  int use_guess;       /* 1: x holds an initial guess on input */
+  int true_residual;   /* 1: check ||b - A x|| / ||b|| with an FP64 matvec at the end */
+} hr_gmres_opts;
+
+typedef struct {
+  int iterations;
+  int restarts;
+  int matvecs_fp64;
+  int matvecs_mixed;
+  double residual;       /* final Arnoldi relative residual */
+  double true_residual;  /* FP64 ||b - A x|| / ||b|| (if requested, else -1) */
+  double seconds;        /* device time of the solve */
+  int guess_rejected;    /* 1 if the initial guess was worse than zero and was dropped */
+  double resid_hist[512];
+} hr_gmres_report;
+
+typedef struct hr_plan2s hr_plan2s;
+
+/* Uploads the scene, builds both treecodes, interaction lists and density
+ * interpolation stencils. Geometry-only work: done once per scene. */
+int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* scene, const hr_eval_opts* opt,
+                     hr_plan2s** out);
+void hr_plan2s_destroy(hr_plan2s* plan);
+/* y = (I - 2/3 D) x (2S/main.cpp:541-677); host buffers of 3(n1+n2). */
+int hr_plan2s_matvec(hr_plan2s* plan, const double* x, double* y);
+/* b = -2/3 S[f] (2S/main.cpp:186-207, 421-537); f1, f2 host 3n_s forces. */
+int hr_plan2s_rhs(hr_plan2s* plan, const double* f1, const double* f2, double* b);
+/* GMRES solve; x in/out (host). */
+int hr_plan2s_solve(hr_plan2s* plan, const hr_gmres_opts* opt, const double* b, double* x,
+                    hr_gmres_report* rep);
+/* Device-pointer variants (buffers already in HBM, on the context's stream). */
+int hr_plan2s_matvec_dev(hr_plan2s* plan, const double* x_dev, double* y_dev, int precision);
+int hr_plan2s_rhs_dev(hr_plan2s* plan, const double* f1_dev, const double* f2_dev, double* b_dev);
+int hr_plan2s_solve_dev(hr_plan2s* plan, const hr_gmres_opts* opt, const double* b_dev,
+                        double* x_dev, hr_gmres_report* rep);
+/* Work counts of one matvec: pair evaluations (direct + proxy), by kind. */
+typedef struct {
+  long long direct_pairs_near; /* regularized (r <= 8 delta candidates) target x source pairs */
+  long long direct_pairs_far;  /* plain-kernel target x source pairs (far targets) */
+  long long proxy_pairs;       /* target x proxy-point evaluations */
+  long long moment_terms;      /* proxy x source terms of the upward pass */
+  long long flops;             /* algorithmic flops by the fixed per-pair convention */
+} hr_work;
+int hr_plan2s_work(hr_plan2s* plan, int which /*0 matvec, 1 rhs*/, hr_work* w);
+/* the plan's stream (cudaStream_t) for callers that enqueue their own work */
+void* hr_plan2s_stream(hr_plan2s* plan);
+/* Times `iters` back-to-back launches of one boundary-sum batch with CUDA
+ * events on the plan's stream (inputs as left by the last matvec / RHS):
+ * which 0 = stresslet batch (matvec, FP64), 1 = Stokeslet batch (RHS),
+ * 2 = stresslet batch (mixed precision). Returns milliseconds per launch. */
+int hr_plan2s_time_batch(hr_plan2s* plan, int which, int iters, double* ms_per_launch);
+
+/* ------------------------------------------- two-surface geometry setup */
+/* Host setup producing an hr_scene2s: Generate_Surface (2S/surface.cpp:13-71),
+ * Compute_nearest_data (2S/surface.cpp:450-526) and surfc_force
+ * (2S/surface.cpp:530-559), parameterized. Default parameters reproduce the
+ * reference's scene (2S/utilities.h:15-26, 2S/utilities.cpp:10-40,
+ * 2S/main.cpp:147-157) bit for bit. */
+typedef struct {
+  double axes[3];       /* spheroid semi-axes (ellipse_a, ellipse_b, ellipse_c) */
+  double center[2][3];  /* centres of surfaces 1 and 2 */
+  double unrot[2][9];   /* row-major "un-rotation" R: body coordinates = R (x - centre) */
+  int rotated[2];       /* 1: the level set uses unrot (the reference's rotated flag) */
+  double kappa0, q;     /* delta = kappa0 (1/64)^(1-q) h^q */
+} hr_geom2s_params;
+
+typedef struct hr_geom2s hr_geom2s;
+int hr_geom2s_default_params(hr_geom2s_params* p);
+/* h = 1/N on the box [-1, 1]^3 around each centre */
+int hr_geom2s_generate(const hr_geom2s_params* p, int N, hr_geom2s** out);
+/* Borrowed views (valid until destroy): the scene and the interfacial force
+ * f = 2 H gamma n - grad_s gamma, gamma = 1 + z^2, at every quadrature point. */
+int hr_geom2s_view(const hr_geom2s* g, hr_scene2s* scene, const double** force);
+void hr_geom2s_destroy(hr_geom2s* g);
+
+/* -------------------------------------------------- measured FP64 peak */
+/* Runs an FP64 FMA throughput loop on the device; returns FLOP/s. */
+int hr_measure_fp64_peak(hr_ctx* ctx, double* flops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
