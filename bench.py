@@ -144,7 +144,6 @@ def run_reference(args, rank, world):
     import numpy as np
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import highreg
     from oracle import Ref2S, ref_available
 
     cores = os.cpu_count()
@@ -155,18 +154,24 @@ def run_reference(args, rank, world):
         line["unavailable"] = "reference build (oracle/_ref) not present on this machine"
         print(json.dumps(line))
         return
-    # pair count of one operator application: same tree decisions as ours
-    geo = highreg.Geometry2S(H_INV).scene
-    n_pairs = None
-    try:
-        ctx = highreg.Context(0)
-        plan = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=P, N0=N0, theta=THETA)
-        n_pairs = pairs_of(plan.work(0))
-        plan.close()
-        ctx.close()
-    except Exception:
-        pass
     R = Ref2S(P, N0).setup(H_INV)
+    # pair count of one operator application (target-source plus target-proxy
+    # evaluations of its four treecode sums), from the checker's statistics on
+    # the reference's own geometry; the count does not depend on the density
+    from oracle import Oracle
+
+    orc = Oracle()
+    geo = R.geometry()
+    n_pairs = 0
+    for s, t in [(0, 0), (0, 1), (1, 0), (1, 1)]:
+        xq, nrm, area = geo["xq%d" % s], geo["nrm%d" % s], geo["area%d" % s]
+        zero = np.zeros(len(xq))
+        if s == t:
+            _, st = orc.kitc(2, P, N0, THETA, geo["ctr%d" % s], R.DEL, xq, nrm, area, zero)
+        else:
+            _, st = orc.kitc(3, P, N0, THETA, geo["ctr%d" % s], R.DEL, xq, nrm, area, zero, xt=geo["xq%d" % t],
+                             b=geo["b%d" % t], x0=geo["x0%d" % t], n0=geo["n0%d" % t], dens0=np.zeros(len(geo["xq%d" % t])))
+        n_pairs += int(st[0] + st[1])
     u = np.random.default_rng(0).standard_normal(3 * sum(R.nq))
     for _ in range(args.warmup):
         R.matvec(u)
@@ -205,6 +210,7 @@ def run_ours(args, rank, world, local_rank):
     f2 = torch.tensor(geo["f1"], dtype=torch.float64, device=dev)
     b = torch.zeros(n, dtype=torch.float64, device=dev)
     x = torch.zeros(n, dtype=torch.float64, device=dev)
+    prec = highreg.HR_MIXED if args.precision == "mixed" else highreg.HR_FP64
     w_rhs = plan.work(1)
     w_mv = plan.work(0)
     stream = torch.cuda.ExternalStream(plan.stream(), device=dev)
@@ -213,7 +219,7 @@ def run_ours(args, rank, world, local_rank):
 
     def step():
         plan.rhs_dev(f1, f2, b)
-        return plan.solve_dev(b, x, restart=RESTART, tol=TOL, precision=highreg.HR_FP64)
+        return plan.solve_dev(b, x, restart=RESTART, tol=TOL, precision=prec)
 
     for _ in range(max(3, args.warmup)):
         rep = step()
@@ -293,12 +299,13 @@ def run_ours(args, rank, world, local_rank):
                 "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (the reference's two-spheroid geometry generated in-process)",
-                "config": {"workload": "two-surface solve h=1/64 (n=%d), KITC P=6 N0=2000 theta=0.6, GMRES restart 50 tol 1e-10, plain FP64" % n,
+                "config": {"workload": "two-surface solve h=1/%d (n=%d), KITC P=6 N0=2000 theta=0.6, GMRES restart 50 tol 1e-10, %s" % (H_INV, n, args.precision),
                            "global_batch": world, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "flushed (256 MB write) before each timed step",
                            "gmres_iterations": it, "matvecs_per_step": mv_per_step,
                            "pairs_per_step": pairs_step, "solve_seconds": t_max / args.steps,
-                           "final_residual": reps[-1]["residual"]},
+                           "final_residual": reps[-1]["residual"], "true_residual": reps[-1]["true_residual"],
+                           "precision": args.precision, "work_matvec": w_mv, "work_rhs": w_rhs},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches}
         print(json.dumps(line))
@@ -314,7 +321,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--h", type=int, default=64, help="1/h of the workload (64 is the benchmark)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
+    global H_INV
+    H_INV = args.h
     rank, world, local_rank = dist_info()
     if world > 1:
         import datetime

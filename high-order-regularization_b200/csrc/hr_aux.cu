@@ -117,13 +117,18 @@ __global__ void moments_reduce_kernel(int C, int Pf, const int* __restrict__ ite
 
 __global__ void permute_kernel(int n, const int* __restrict__ perm, const double* __restrict__ q3,
                                double* __restrict__ qx, double* __restrict__ qy,
-                               double* __restrict__ qz) {
+                               double* __restrict__ qz, float* __restrict__ fqx,
+                               float* __restrict__ fqy, float* __restrict__ fqz) {
   int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   int o = perm[p];
-  qx[p] = q3[3 * o];
-  qy[p] = q3[3 * o + 1];
-  qz[p] = q3[3 * o + 2];
+  const double a = q3[3 * o], b = q3[3 * o + 1], c = q3[3 * o + 2];
+  qx[p] = a;
+  qy[p] = b;
+  qz[p] = c;
+  fqx[p] = (float)a;
+  fqy[p] = (float)b;
+  fqz[p] = (float)c;
 }
 
 __global__ void permute_soa_kernel(int n, const int* __restrict__ perm,
@@ -301,9 +306,9 @@ void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_star
 }
 
 void launch_permute(int n, const int* perm, const double* q3, double* qx, double* qy, double* qz,
-                    cudaStream_t st) {
+                    float* fqx, float* fqy, float* fqz, cudaStream_t st) {
   if (n <= 0) return;
-  permute_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, perm, q3, qx, qy, qz);
+  permute_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, perm, q3, qx, qy, qz, fqx, fqy, fqz);
 }
 
 void launch_permute_soa(int n, const int* perm, const double* src, double* dst, cudaStream_t st) {

@@ -181,6 +181,7 @@ void single_eval(Ctx& C, int kind, const hr_eval_opts* opt, double delta, const 
   }
   EvalTask task = make_task(kind, delta, scale, tree, L, tg, d_out.p);
   task.jump_mode = direct ? 1 : 0;
+  task.mixed = (opt && opt->precision == HR_MIXED) ? 1 : 0;
   if (on) task.tq = q3.p;
   Batch B;
   B.family = dl ? F_DL : ((kind <= K_DL_OFF) ? F_SL : F_E2G);

@@ -22,6 +22,9 @@ struct EvalTask {
   double scale;   // final factor of the sum (1/8pi, -6/8pi, ...)
   const double *sx, *sy, *sz, *snx, *sny, *snz, *sa;  // sources, tree order
   const double *qx, *qy, *qz;                         // density, tree order
+  double ctr[3];                                      // source surface centre (FP32 frame origin)
+  // FP32 copies for the mixed-precision far field: positions relative to ctr
+  const float *fx, *fy, *fz, *fnx, *fny, *fnz, *fa, *fqx, *fqy, *fqz;
   const int *node_m0, *node_m1;                       // inclusive member ranges
   const double* tcheb;                                // 3*P1 per node
   const double* mom;                                  // C*Pf per node
@@ -47,7 +50,7 @@ enum Family : int { F_SL = 0, F_DL = 1, F_E2G = 2 };
 
 // Evaluates every block of a combined block list in one launch.
 void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_blocks, int nblocks,
-                 cudaStream_t st);
+                 cudaStream_t st, bool mixed);
 
 // Upward pass: proxy moments of every non-root node of a tree.
 struct MomItem {
@@ -65,7 +68,7 @@ void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_star
 
 // Gathers interleaved reference-order density into tree-order SoA.
 void launch_permute(int n, const int* perm, const double* q3, double* qx, double* qy, double* qz,
-                    cudaStream_t st);
+                    float* fqx, float* fqy, float* fqz, cudaStream_t st);
 void launch_permute_soa(int n, const int* perm, const double* src, double* dst, cudaStream_t st);
 
 // Six-point density interpolation at nearest points.

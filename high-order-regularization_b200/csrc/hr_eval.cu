@@ -6,13 +6,19 @@
 //   * near entry  -> direct sum over the node's member sources, staged in
 //                    shared memory in tiles of 256 (Call_Ds_*, 2S/KITC.cpp:807-1062;
 //                    in direct mode the single node holds all sources, i.e.
-//                    eval_Stokes_*_{on,off}Surf, 2S/stokeslets.cpp, 2S/stresslets.cpp,
-//                    and the E2G sums of E2G/stokes.cpp);
+//                    eval_Stokes_*_{on,off}Surf of 2S/stokeslets.cpp and
+//                    2S/stresslets.cpp, and the sums of E2G/stokes.cpp);
 //   * far entry   -> the node's (P+1)^3 proxy points with their moments staged
 //                    in shared memory (Call_Treecode_*, 2S/KITC.cpp:671-777).
 // A warp whose mask word is zero for an entry skips the arithmetic entirely.
-// The per-pair formulas are those of hr_pairs.cuh; the per-target epilogues
-// (scale and jump terms) are those of the reference drivers cited below.
+//
+// Precision. FP64: every pair in FP64. MIXED: pairs that are well separated
+// in the reference's own sense (every pair of a target with |b|/delta > 8, the
+// r > 8 delta pairs of targets that use the regularized kernels, and all
+// proxy interactions) are evaluated in FP32 from centre-relative FP32
+// coordinates, summed per tile in FP32 and added to the FP64 per-target
+// accumulators; the r <= 8 delta pairs (erf/exp smoothing, subtraction) and
+// every pair of a near off-surface stresslet target stay in FP64.
 #include <cstdio>
 
 #include "hr_device.h"
@@ -22,8 +28,8 @@ namespace hr {
 
 namespace {
 
-constexpr int kNT = 256;               // sources per shared-memory tile
-constexpr int kSmem = 10 * kNT;        // doubles: 10 SoA arrays of a source tile
+constexpr int kNT = 256;         // sources per shared-memory tile
+constexpr int kSmem = 10 * kNT;  // doubles: 10 SoA arrays of a source tile
 constexpr int kMaxP1 = 16;
 
 struct Tgt {
@@ -36,8 +42,16 @@ struct Tgt {
   Coef c;
 };
 
+struct Tgt32 {
+  float px, py, pz;  // relative to the source surface centre
+  float f0n0;        // 0 for targets without subtraction
+  float g0[3];
+  float n0xf0[3];
+};
+
 template <int KIND>
-__device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid, Tgt& S) {
+__device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid, Tgt& S,
+                                            Tgt32& F) {
   S.px = S.py = S.pz = 0.0;
   S.b = 0.0;
   S.f0n0 = 0.0;
@@ -45,54 +59,64 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
   S.c.c1 = S.c.c2 = S.c.c3 = 0.0;
   // regularized-kernel kinds: on-surface sums and the E2G band sums
   S.near = (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_E2G_SL7 || KIND == K_E2G_P7) ? 1 : 0;
-  if (!valid) return;
-  S.px = T.txyz[3 * t];
-  S.py = T.txyz[3 * t + 1];
-  S.pz = T.txyz[3 * t + 2];
-  if (KIND == K_SL_ON) {
-    // f0_dot_n0 = Surfc[i].f . Surfc[i].Nrml  (2S/KITC.cpp:1461, 2S/stokeslets.cpp:167)
-    S.f0n0 = T.tq[3 * t] * T.tnrm[3 * t] + T.tq[3 * t + 1] * T.tnrm[3 * t + 1] +
-             T.tq[3 * t + 2] * T.tnrm[3 * t + 2];
-  } else if (KIND == K_SL_OFF || KIND == K_E2G_SL7) {
-    S.b = T.tb[t];
-    S.near = T.tnear[t];
-    // f0_dot_n0 = nrst_f . nrst_Nrml  (2S/KITC.cpp:1568, E2G/main.cpp:1338)
-    S.f0n0 = T.tf0[3 * t] * T.tn0[3 * t] + T.tf0[3 * t + 1] * T.tn0[3 * t + 1] +
-             T.tf0[3 * t + 2] * T.tn0[3 * t + 2];
-    if (S.near) S.c = reg_coeff(S.b / T.DEL);
-  } else if (KIND == K_DL_ON) {
-    for (int k = 0; k < 3; k++) S.g0[k] = T.tq[3 * t + k];
-  } else if (KIND == K_DL_OFF) {
-    S.b = T.tb[t];
-    S.near = T.tnear[t];
-    for (int k = 0; k < 3; k++) {
-      S.x0[k] = T.tx0[3 * t + k];
-      S.n0[k] = T.tn0[3 * t + k];
-      S.g0[k] = T.tg0[3 * t + k];
+  if (valid) {
+    S.px = T.txyz[3 * t];
+    S.py = T.txyz[3 * t + 1];
+    S.pz = T.txyz[3 * t + 2];
+    if (KIND == K_SL_ON) {
+      // f0_dot_n0 = Surfc[i].f . Surfc[i].Nrml  (2S/KITC.cpp:1461, 2S/stokeslets.cpp:167)
+      S.f0n0 = T.tq[3 * t] * T.tnrm[3 * t] + T.tq[3 * t + 1] * T.tnrm[3 * t + 1] +
+               T.tq[3 * t + 2] * T.tnrm[3 * t + 2];
+    } else if (KIND == K_SL_OFF || KIND == K_E2G_SL7) {
+      S.b = T.tb[t];
+      if (KIND == K_SL_OFF) S.near = T.tnear[t];
+      // f0_dot_n0 = nrst_f . nrst_Nrml  (2S/KITC.cpp:1568, E2G/main.cpp:1338)
+      S.f0n0 = T.tf0[3 * t] * T.tn0[3 * t] + T.tf0[3 * t + 1] * T.tn0[3 * t + 1] +
+               T.tf0[3 * t + 2] * T.tn0[3 * t + 2];
+      if (S.near) S.c = reg_coeff(S.b / T.DEL);
+    } else if (KIND == K_DL_ON) {
+      for (int k = 0; k < 3; k++) S.g0[k] = T.tq[3 * t + k];
+    } else if (KIND == K_DL_OFF) {
+      S.b = T.tb[t];
+      S.near = T.tnear[t];
+      for (int k = 0; k < 3; k++) {
+        S.x0[k] = T.tx0[3 * t + k];
+        S.n0[k] = T.tn0[3 * t + k];
+        S.g0[k] = T.tg0[3 * t + k];
+      }
+      if (S.near) S.c = reg_coeff(S.b / T.DEL);
+    } else if (KIND == K_E2G_P7) {
+      S.b = T.tb[t];
+      double f0[3], n0[3];
+      for (int k = 0; k < 3; k++) {
+        f0[k] = T.tf0[3 * t + k];
+        n0[k] = T.tn0[3 * t + k];
+      }
+      // E2G/stokes.cpp:144-145
+      S.f0n0 = f0[0] * n0[0] + f0[1] * n0[1] + f0[2] * n0[2];
+      S.n0xf0[0] = n0[1] * f0[2] - n0[2] * f0[1];
+      S.n0xf0[1] = n0[2] * f0[0] - n0[0] * f0[2];
+      S.n0xf0[2] = n0[0] * f0[1] - n0[1] * f0[0];
+      S.c = reg_coeff(S.b / T.DEL);
     }
-    if (S.near) S.c = reg_coeff(S.b / T.DEL);
-  } else if (KIND == K_E2G_P7) {
-    S.b = T.tb[t];
-    double f0[3], n0[3];
-    for (int k = 0; k < 3; k++) {
-      f0[k] = T.tf0[3 * t + k];
-      n0[k] = T.tn0[3 * t + k];
-    }
-    // E2G/stokes.cpp:144-145
-    S.f0n0 = f0[0] * n0[0] + f0[1] * n0[1] + f0[2] * n0[2];
-    S.n0xf0[0] = n0[1] * f0[2] - n0[2] * f0[1];
-    S.n0xf0[1] = n0[2] * f0[0] - n0[0] * f0[2];
-    S.n0xf0[2] = n0[0] * f0[1] - n0[1] * f0[0];
-    S.c = reg_coeff(S.b / T.DEL);
+  }
+  F.px = (float)(S.px - T.ctr[0]);
+  F.py = (float)(S.py - T.ctr[1]);
+  F.pz = (float)(S.pz - T.ctr[2]);
+  // the direct sum of a far Stokeslet target has no subtraction (2S/KITC.cpp:856-882)
+  F.f0n0 = (KIND == K_SL_OFF && !S.near) ? 0.0f : (float)S.f0n0;
+  for (int k = 0; k < 3; k++) {
+    F.g0[k] = (float)S.g0[k];
+    F.n0xf0[k] = (float)S.n0xf0[k];
   }
 }
 
-// Direct sum of one staged tile for one target.
+// ---------------------------------------------------------------- FP64 pairs
+
+// One FP64 pair; returns true if the smoothed (erf) branch was taken.
 template <int KIND>
-__device__ __forceinline__ void tile_pairs(const double* __restrict__ sm, int cnt, double DEL,
-                                           double d64, const Tgt& S, double& a0, double& a1,
-                                           double& a2, unsigned long long& creg,
-                                           unsigned long long& cplain) {
+__device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, const Tgt& S,
+                                       const Reg& g, double& a0, double& a1, double& a2) {
   const double* X = sm;
   const double* Y = sm + kNT;
   const double* Z = sm + 2 * kNT;
@@ -103,222 +127,211 @@ __device__ __forceinline__ void tile_pairs(const double* __restrict__ sm, int cn
   const double* QX = sm + 7 * kNT;
   const double* QY = sm + 8 * kNT;
   const double* QZ = sm + 9 * kNT;
-  if (KIND == K_SL_ON) {
-    // Call_Ds_SL_onSurf (2S/KITC.cpp:807-844)
-    for (int j = 0; j < cnt; j++) {
-      double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-      double r2 = dx * dx + dy * dy + dz * dz;
-      double r = sqrt(r2);
-      double area = A[j];
-      double fx = QX[j] - S.f0n0 * NX[j];
-      double fy = QY[j] - S.f0n0 * NY[j];
-      double fz = QZ[j] - S.f0n0 * NZ[j];
-      double fdd = fx * dx + fy * dy + fz * dz;
-      double H1, H2;
-      sl_7ord_onsurf(r, DEL, H1, H2);
-      creg += (r2 <= d64);
-      H1 *= area;
-      H2 *= area * fdd;
-      a0 += fx * H1 + dx * H2;
-      a1 += fy * H1 + dy * H2;
-      a2 += fz * H1 + dz * H2;
-    }
-    cplain += cnt;
-  } else if (KIND == K_SL_OFF || KIND == K_E2G_SL7) {
-    if (S.near) {
-      // Call_Ds_SL regularized branch (2S/KITC.cpp:883-915), stokes_SL_7ord
-      for (int j = 0; j < cnt; j++) {
-        double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-        double r2 = dx * dx + dy * dy + dz * dz;
-        double r = sqrt(r2);
-        double area = A[j];
-        double fx = QX[j] - S.f0n0 * NX[j];
-        double fy = QY[j] - S.f0n0 * NY[j];
-        double fz = QZ[j] - S.f0n0 * NZ[j];
-        double fdd = fx * dx + fy * dy + fz * dz;
-        double H1, H2;
-        sl_7ord(r, DEL, S.c, H1, H2);
-        creg += (r2 <= d64);
-        H1 *= area;
-        H2 *= fdd * area;
-        a0 += fx * H1 + dx * H2;
-        a1 += fy * H1 + dy * H2;
-        a2 += fz * H1 + dz * H2;
-      }
-    } else {
-      // far target: plain Stokeslet without subtraction (2S/KITC.cpp:856-882)
-      for (int j = 0; j < cnt; j++) {
-        double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-        double r2 = dx * dx + dy * dy + dz * dz;
-        double r = sqrt(r2);
-        double area = A[j];
-        double fx = QX[j], fy = QY[j], fz = QZ[j];
-        double fdd = fx * dx + fy * dy + fz * dz;
-        double H1 = area / r;
-        double H2 = fdd * area / (r2 * r);
-        a0 += fx * H1 + dx * H2;
-        a1 += fy * H1 + dy * H2;
-        a2 += fz * H1 + dz * H2;
-      }
-    }
-    cplain += cnt;
+  const double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  const double rinv = rsqrt(r2);
+  bool reg = false;
+  if (KIND == K_SL_ON || ((KIND == K_SL_OFF || KIND == K_E2G_SL7) && S.near)) {
+    // Call_Ds_SL_onSurf / Call_Ds_SL regularized branch / stokes_SL_7ord
+    const double area = A[j];
+    const double fx = QX[j] - S.f0n0 * NX[j];
+    const double fy = QY[j] - S.f0n0 * NY[j];
+    const double fz = QZ[j] - S.f0n0 * NZ[j];
+    const double fdd = fx * dx + fy * dy + fz * dz;
+    double H1, H2;
+    if (KIND == K_SL_ON) reg = sl_7ord_onsurf(r2, rinv, g, H1, H2);
+    else reg = sl_7ord(r2, rinv, g, S.c, H1, H2);
+    H1 *= area;
+    H2 *= area * fdd;
+    a0 += fx * H1 + dx * H2;
+    a1 += fy * H1 + dy * H2;
+    a2 += fz * H1 + dz * H2;
+  } else if (KIND == K_SL_OFF || KIND == K_E2G_SL_AWAY) {
+    // plain Stokeslet without subtraction (2S/KITC.cpp:856-882, E2G/stokes.cpp:22-40)
+    const double fx = QX[j], fy = QY[j], fz = QZ[j];
+    const double fdd = fx * dx + fy * dy + fz * dz;
+    const double H1 = A[j] * rinv;
+    const double H2 = fdd * H1 * (rinv * rinv);
+    a0 += fx * H1 + dx * H2;
+    a1 += fy * H1 + dy * H2;
+    a2 += fz * H1 + dz * H2;
   } else if (KIND == K_DL_ON) {
     // Call_Ds_DL_onSurf (2S/KITC.cpp:921-957)
-    for (int j = 0; j < cnt; j++) {
-      double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-      double r2 = dx * dx + dy * dy + dz * dz;
-      double r = sqrt(r2);
-      double gx = QX[j] - S.g0[0];
-      double gy = QY[j] - S.g0[1];
-      double gz = QZ[j] - S.g0[2];
-      double gdd = gx * dx + gy * dy + gz * dz;
-      double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
-      double H3 = dl_7ord_onsurf(r, DEL);
-      creg += (r2 <= d64);
-      double kernel = ndd * gdd * H3 * A[j];
-      a0 += dx * kernel;
-      a1 += dy * kernel;
-      a2 += dz * kernel;
-    }
-    cplain += cnt;
+    const double gx = QX[j] - S.g0[0];
+    const double gy = QY[j] - S.g0[1];
+    const double gz = QZ[j] - S.g0[2];
+    const double gdd = gx * dx + gy * dy + gz * dz;
+    const double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+    double H3;
+    reg = dl_7ord_onsurf(r2, rinv, g, H3);
+    const double kernel = ndd * gdd * H3 * A[j];
+    a0 += dx * kernel;
+    a1 += dy * kernel;
+    a2 += dz * kernel;
   } else if (KIND == K_DL_OFF) {
     if (S.near) {
       // Call_Ds_DL regularized branch (2S/KITC.cpp:996-1059), stokes_DL_7ord
       const double b = S.b;
-      for (int j = 0; j < cnt; j++) {
-        double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-        double r2 = dx * dx + dy * dy + dz * dz;
-        double r = sqrt(r2);
-        double xh0 = X[j] - S.x0[0];
-        double xh1 = Y[j] - S.x0[1];
-        double xh2 = Z[j] - S.x0[2];
-        double gx = QX[j] - S.g0[0];
-        double gy = QY[j] - S.g0[1];
-        double gz = QZ[j] - S.g0[2];
-        double sig_sq = (xh0 * xh0 + xh1 * xh1 + xh2 * xh2) -
-                        2.0 * b * (xh0 * S.n0[0] + xh1 * S.n0[1] + xh2 * S.n0[2]);
-        double g_dot_n0 = gx * S.n0[0] + gy * S.n0[1] + gz * S.n0[2];
-        double g_dot_xh = gx * xh0 + gy * xh1 + gz * xh2;
-        double n0_dot_n = S.n0[0] * NX[j] + S.n0[1] * NY[j] + S.n0[2] * NZ[j];
-        double xh_dot_n = xh0 * NX[j] + xh1 * NY[j] + xh2 * NZ[j];
-        double c_m1a = g_dot_n0 * n0_dot_n;
-        double c_m1b = g_dot_xh * n0_dot_n + g_dot_n0 * xh_dot_n;
-        double c_m2a = g_dot_xh * xh_dot_n;
-        double c_m2b = b * c_m1b;
-        double H2, H3;
-        dl_7ord(r, DEL, S.c, H2, H3);
-        creg += (r2 <= d64);
-        double area = A[j];
-        H2 *= area;
-        H3 *= area;
-        double m1 = dx * c_m1a - S.n0[0] * c_m1b;
-        double m2 = -sig_sq * m1 + dx * c_m2a + xh0 * c_m2b;
-        a0 += m1 * H2 + m2 * H3;
-        m1 = dy * c_m1a - S.n0[1] * c_m1b;
-        m2 = -sig_sq * m1 + dy * c_m2a + xh1 * c_m2b;
-        a1 += m1 * H2 + m2 * H3;
-        m1 = dz * c_m1a - S.n0[2] * c_m1b;
-        m2 = -sig_sq * m1 + dz * c_m2a + xh2 * c_m2b;
-        a2 += m1 * H2 + m2 * H3;
-      }
+      const double xh0 = X[j] - S.x0[0];
+      const double xh1 = Y[j] - S.x0[1];
+      const double xh2 = Z[j] - S.x0[2];
+      const double gx = QX[j] - S.g0[0];
+      const double gy = QY[j] - S.g0[1];
+      const double gz = QZ[j] - S.g0[2];
+      const double sig_sq = (xh0 * xh0 + xh1 * xh1 + xh2 * xh2) -
+                            2.0 * b * (xh0 * S.n0[0] + xh1 * S.n0[1] + xh2 * S.n0[2]);
+      const double g_dot_n0 = gx * S.n0[0] + gy * S.n0[1] + gz * S.n0[2];
+      const double g_dot_xh = gx * xh0 + gy * xh1 + gz * xh2;
+      const double n0_dot_n = S.n0[0] * NX[j] + S.n0[1] * NY[j] + S.n0[2] * NZ[j];
+      const double xh_dot_n = xh0 * NX[j] + xh1 * NY[j] + xh2 * NZ[j];
+      const double c_m1a = g_dot_n0 * n0_dot_n;
+      const double c_m1b = g_dot_xh * n0_dot_n + g_dot_n0 * xh_dot_n;
+      const double c_m2a = g_dot_xh * xh_dot_n;
+      const double c_m2b = b * c_m1b;
+      double H2, H3;
+      reg = dl_7ord(r2, rinv, g, S.c, H2, H3);
+      const double area = A[j];
+      H2 *= area;
+      H3 *= area;
+      double m1 = dx * c_m1a - S.n0[0] * c_m1b;
+      double m2 = -sig_sq * m1 + dx * c_m2a + xh0 * c_m2b;
+      a0 += m1 * H2 + m2 * H3;
+      m1 = dy * c_m1a - S.n0[1] * c_m1b;
+      m2 = -sig_sq * m1 + dy * c_m2a + xh1 * c_m2b;
+      a1 += m1 * H2 + m2 * H3;
+      m1 = dz * c_m1a - S.n0[2] * c_m1b;
+      m2 = -sig_sq * m1 + dz * c_m2a + xh2 * c_m2b;
+      a2 += m1 * H2 + m2 * H3;
     } else {
-      // far target: plain stresslet (2S/KITC.cpp:970-995)
-      for (int j = 0; j < cnt; j++) {
-        double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-        double r2 = dx * dx + dy * dy + dz * dz;
-        double r = sqrt(r2);
-        double gdd = QX[j] * dx + QY[j] * dy + QZ[j] * dz;
-        double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
-        double kernel = gdd * ndd / (r2 * r2 * r) * A[j];
-        a0 += dx * kernel;
-        a1 += dy * kernel;
-        a2 += dz * kernel;
-      }
+      // plain stresslet (2S/KITC.cpp:970-995)
+      const double gdd = QX[j] * dx + QY[j] * dy + QZ[j] * dz;
+      const double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+      const double rinv2 = rinv * rinv;
+      const double kernel = gdd * ndd * (rinv2 * rinv2 * rinv) * A[j];
+      a0 += dx * kernel;
+      a1 += dy * kernel;
+      a2 += dz * kernel;
     }
-    cplain += cnt;
-  } else if (KIND == K_E2G_SL_AWAY) {
-    // stokes_SL_away (E2G/stokes.cpp:22-40)
-    for (int j = 0; j < cnt; j++) {
-      double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-      double r2 = dx * dx + dy * dy + dz * dz;
-      double fdd = QX[j] * dx + QY[j] * dy + QZ[j] * dz;
-      double H1 = 1.0 / sqrt(r2) * A[j];
-      double H2 = H1 / r2 * fdd;
-      a0 += QX[j] * H1 + dx * H2;
-      a1 += QY[j] * H1 + dy * H2;
-      a2 += QZ[j] * H1 + dz * H2;
-    }
-    cplain += cnt;
   } else if (KIND == K_E2G_P_AWAY) {
     // stokes_pressure_away (E2G/stokes.cpp:108-121)
-    for (int j = 0; j < cnt; j++) {
-      double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-      double r2 = dx * dx + dy * dy + dz * dz;
-      double H2 = 1.0 / (r2 * sqrt(r2));
-      H2 *= QX[j] * dx + QY[j] * dy + QZ[j] * dz;
-      a0 += H2 * A[j];
-    }
-    cplain += cnt;
+    const double H2 = (QX[j] * dx + QY[j] * dy + QZ[j] * dz) * (rinv * rinv * rinv);
+    a0 += H2 * A[j];
   } else if (KIND == K_E2G_P7) {
     // stokes_pressure_7ord (E2G/stokes.cpp:151-194)
-    for (int j = 0; j < cnt; j++) {
-      double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
-      double r2 = dx * dx + dy * dy + dz * dz;
-      double r = sqrt(r2);
-      double H2 = lapl_dl_7ord(r, DEL, S.c);
-      creg += (r2 <= d64);
-      double n0 = NX[j], n1 = NY[j], n2 = NZ[j];
-      double f0 = QX[j], f1 = QY[j], f2 = QZ[j];
-      double f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
-      double ncf0 = (n1 * f2 - n2 * f1) - S.n0xf0[0];
-      double ncf1 = (n2 * f0 - n0 * f2) - S.n0xf0[1];
-      double ncf2 = (n0 * f1 - n1 * f0) - S.n0xf0[2];
-      double n_dot_dx = n0 * dx + n1 * dy + n2 * dz;
-      double ncd0 = n1 * dz - n2 * dy;
-      double ncd1 = n2 * dx - n0 * dz;
-      double ncd2 = n0 * dy - n1 * dx;
-      double normal = -(f_dot_n - S.f0n0) * n_dot_dx;
-      double tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
-      a0 += (normal + tangential) * H2 * A[j];
-    }
-    cplain += cnt;
+    double H2;
+    reg = lapl_dl_7ord(r2, rinv, g, S.c, H2);
+    const double n0 = NX[j], n1 = NY[j], n2 = NZ[j];
+    const double f0 = QX[j], f1 = QY[j], f2 = QZ[j];
+    const double f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
+    const double ncf0 = (n1 * f2 - n2 * f1) - S.n0xf0[0];
+    const double ncf1 = (n2 * f0 - n0 * f2) - S.n0xf0[1];
+    const double ncf2 = (n0 * f1 - n1 * f0) - S.n0xf0[2];
+    const double n_dot_dx = n0 * dx + n1 * dy + n2 * dz;
+    const double ncd0 = n1 * dz - n2 * dy;
+    const double ncd1 = n2 * dx - n0 * dz;
+    const double ncd2 = n0 * dy - n1 * dx;
+    const double normal = -(f_dot_n - S.f0n0) * n_dot_dx;
+    const double tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
+    a0 += (normal + tangential) * H2 * A[j];
+  }
+  return reg;
+}
+
+// ------------------------------------------------------- FP32 plain pairs
+// The singular kernel of each kind (the r/delta > 8 branch of the reference),
+// from FP32 centre-relative coordinates.
+template <int KIND>
+__device__ __forceinline__ void pair32(const float* __restrict__ sf, int j, const Tgt32& F,
+                                       float& p0, float& p1, float& p2) {
+  const float* X = sf;
+  const float* Y = sf + kNT;
+  const float* Z = sf + 2 * kNT;
+  const float* NX = sf + 3 * kNT;
+  const float* NY = sf + 4 * kNT;
+  const float* NZ = sf + 5 * kNT;
+  const float* A = sf + 6 * kNT;
+  const float* QX = sf + 7 * kNT;
+  const float* QY = sf + 8 * kNT;
+  const float* QZ = sf + 9 * kNT;
+  const float dx = F.px - X[j], dy = F.py - Y[j], dz = F.pz - Z[j];
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = rsqrtf(r2);
+  const float rinv2 = rinv * rinv;
+  if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7 || KIND == K_E2G_SL_AWAY) {
+    const float fx = QX[j] - F.f0n0 * NX[j];
+    const float fy = QY[j] - F.f0n0 * NY[j];
+    const float fz = QZ[j] - F.f0n0 * NZ[j];
+    const float fdd = fx * dx + fy * dy + fz * dz;
+    const float H1 = A[j] * rinv;
+    const float H2 = fdd * H1 * rinv2;
+    p0 += fx * H1 + dx * H2;
+    p1 += fy * H1 + dy * H2;
+    p2 += fz * H1 + dz * H2;
+  } else if (KIND == K_DL_ON || KIND == K_DL_OFF) {
+    const float gx = QX[j] - F.g0[0];
+    const float gy = QY[j] - F.g0[1];
+    const float gz = QZ[j] - F.g0[2];
+    const float gdd = gx * dx + gy * dy + gz * dz;
+    const float ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+    const float kernel = ndd * gdd * (rinv2 * rinv2 * rinv) * A[j];
+    p0 += dx * kernel;
+    p1 += dy * kernel;
+    p2 += dz * kernel;
+  } else if (KIND == K_E2G_P_AWAY) {
+    p0 += (QX[j] * dx + QY[j] * dy + QZ[j] * dz) * (rinv2 * rinv) * A[j];
+  } else if (KIND == K_E2G_P7) {
+    const float n0 = NX[j], n1 = NY[j], n2 = NZ[j];
+    const float f0 = QX[j], f1 = QY[j], f2 = QZ[j];
+    const float f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
+    const float ncf0 = (n1 * f2 - n2 * f1) - F.n0xf0[0];
+    const float ncf1 = (n2 * f0 - n0 * f2) - F.n0xf0[1];
+    const float ncf2 = (n0 * f1 - n1 * f0) - F.n0xf0[2];
+    const float n_dot_dx = n0 * dx + n1 * dy + n2 * dz;
+    const float ncd0 = n1 * dz - n2 * dy;
+    const float ncd1 = n2 * dx - n0 * dz;
+    const float ncd2 = n0 * dy - n1 * dx;
+    const float normal = -(f_dot_n - F.f0n0) * n_dot_dx;
+    const float tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
+    p0 += (normal + tangential) * (rinv2 * rinv) * A[j];
   }
 }
 
-// Proxy-point (far-field) sum of one staged moment tile.
+// ------------------------------------------------------------ proxy tiles
+
 template <bool DL>
-__device__ __forceinline__ void tile_proxies(const double* __restrict__ sm, int PT, int cnt,
-                                             int kk0, int P1, const double* __restrict__ cheb,
-                                             const Tgt& S, double& a0, double& a1, double& a2) {
+__device__ __forceinline__ void proxies64(const double* __restrict__ sm, int PT, int cnt, int kk0,
+                                          int P1, const double* __restrict__ cheb, const Tgt& S,
+                                          double& a0, double& a1, double& a2) {
   int rem = kk0 % (P1 * P1);
   int pi = kk0 / (P1 * P1), pj = rem / P1, pk = rem % P1;
   for (int i = 0; i < cnt; i++) {
-    double dx0 = S.px - cheb[pi];
-    double dx1 = S.py - cheb[P1 + pj];
-    double dx2 = S.pz - cheb[2 * P1 + pk];
-    double r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
-    double r = sqrt(r2);
+    const double dx0 = S.px - cheb[pi];
+    const double dx1 = S.py - cheb[P1 + pj];
+    const double dx2 = S.pz - cheb[2 * P1 + pk];
+    const double r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+    const double rinv = rsqrt(r2);
+    const double rinv2 = rinv * rinv;
     if (!DL) {
       // Call_Treecode_SL (2S/KITC.cpp:700-714)
-      double m0 = sm[i] - S.f0n0 * sm[3 * PT + i];
-      double m1 = sm[PT + i] - S.f0n0 * sm[4 * PT + i];
-      double m2 = sm[2 * PT + i] - S.f0n0 * sm[5 * PT + i];
-      double temp = (m0 * dx0 + m1 * dx1 + m2 * dx2) / (r2 * r);
-      a0 += m0 / r + temp * dx0;
-      a1 += m1 / r + temp * dx1;
-      a2 += m2 / r + temp * dx2;
+      const double m0 = sm[i] - S.f0n0 * sm[3 * PT + i];
+      const double m1 = sm[PT + i] - S.f0n0 * sm[4 * PT + i];
+      const double m2 = sm[2 * PT + i] - S.f0n0 * sm[5 * PT + i];
+      const double temp = (m0 * dx0 + m1 * dx1 + m2 * dx2) * (rinv2 * rinv);
+      a0 += m0 * rinv + temp * dx0;
+      a1 += m1 * rinv + temp * dx1;
+      a2 += m2 * rinv + temp * dx2;
     } else {
       // Call_Treecode_DL (2S/KITC.cpp:753-771)
-      double M9 = sm[9 * PT + i], M10 = sm[10 * PT + i], M11 = sm[11 * PT + i];
+      const double M9 = sm[9 * PT + i], M10 = sm[10 * PT + i], M11 = sm[11 * PT + i];
       double tl[3];
 #pragma unroll
       for (int l = 0; l < 3; l++) {
-        double ta = sm[(3 * l) * PT + i] - S.g0[l] * M9;
-        double tb = sm[(3 * l + 1) * PT + i] - S.g0[l] * M10;
-        double tc = sm[(3 * l + 2) * PT + i] - S.g0[l] * M11;
+        const double ta = sm[(3 * l) * PT + i] - S.g0[l] * M9;
+        const double tb = sm[(3 * l + 1) * PT + i] - S.g0[l] * M10;
+        const double tc = sm[(3 * l + 2) * PT + i] - S.g0[l] * M11;
         tl[l] = ta * dx0 + tb * dx1 + tc * dx2;
       }
-      double kernel = (tl[0] * dx0 + tl[1] * dx1 + tl[2] * dx2) / (r2 * r2 * r);
+      const double kernel = (tl[0] * dx0 + tl[1] * dx1 + tl[2] * dx2) * (rinv2 * rinv2 * rinv);
       a0 += dx0 * kernel;
       a1 += dx1 * kernel;
       a2 += dx2 * kernel;
@@ -333,20 +346,73 @@ __device__ __forceinline__ void tile_proxies(const double* __restrict__ sm, int 
   }
 }
 
-template <int KIND>
-__device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm, double* cheb) {
+template <bool DL>
+__device__ __forceinline__ void proxies32(const float* __restrict__ sf, int PT, int cnt, int kk0,
+                                          int P1, const float* __restrict__ chebf, const Tgt32& F,
+                                          float& p0, float& p1, float& p2) {
+  int rem = kk0 % (P1 * P1);
+  int pi = kk0 / (P1 * P1), pj = rem / P1, pk = rem % P1;
+  for (int i = 0; i < cnt; i++) {
+    const float dx0 = F.px - chebf[pi];
+    const float dx1 = F.py - chebf[P1 + pj];
+    const float dx2 = F.pz - chebf[2 * P1 + pk];
+    const float r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
+    const float rinv = rsqrtf(r2);
+    const float rinv2 = rinv * rinv;
+    if (!DL) {
+      const float m0 = sf[i] - F.f0n0 * sf[3 * PT + i];
+      const float m1 = sf[PT + i] - F.f0n0 * sf[4 * PT + i];
+      const float m2 = sf[2 * PT + i] - F.f0n0 * sf[5 * PT + i];
+      const float temp = (m0 * dx0 + m1 * dx1 + m2 * dx2) * (rinv2 * rinv);
+      p0 += m0 * rinv + temp * dx0;
+      p1 += m1 * rinv + temp * dx1;
+      p2 += m2 * rinv + temp * dx2;
+    } else {
+      const float M9 = sf[9 * PT + i], M10 = sf[10 * PT + i], M11 = sf[11 * PT + i];
+      float tl[3];
+#pragma unroll
+      for (int l = 0; l < 3; l++) {
+        const float ta = sf[(3 * l) * PT + i] - F.g0[l] * M9;
+        const float tb = sf[(3 * l + 1) * PT + i] - F.g0[l] * M10;
+        const float tc = sf[(3 * l + 2) * PT + i] - F.g0[l] * M11;
+        tl[l] = ta * dx0 + tb * dx1 + tc * dx2;
+      }
+      const float kernel = (tl[0] * dx0 + tl[1] * dx1 + tl[2] * dx2) * (rinv2 * rinv2 * rinv);
+      p0 += dx0 * kernel;
+      p1 += dx1 * kernel;
+      p2 += dx2 * kernel;
+    }
+    if (++pk == P1) {
+      pk = 0;
+      if (++pj == P1) {
+        pj = 0;
+        ++pi;
+      }
+    }
+  }
+}
+
+template <int KIND, bool MIXED>
+__device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm, float* sf,
+                                          double* cheb, float* chebf) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int k = blk * kTB + tid;
   const bool valid = k < T.nt;
   const int t = valid ? T.tord[k] : 0;
   Tgt S;
-  load_target<KIND>(T, t, valid, S);
-  const double DEL = T.DEL;
-  const double d64 = 64.0 * DEL * DEL;
+  Tgt32 F;
+  load_target<KIND>(T, t, valid, S, F);
+  const Reg g = make_reg(T.DEL);
+  const float d64f = (float)g.d64;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   unsigned long long creg = 0, cplain = 0, cfar = 0, cprox = 0;
   const int e0 = T.blk_start[blk], e1 = T.blk_start[blk + 1];
   constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY);
+  // which path a target takes through a source tile
+  constexpr bool kPerPairSplit =
+      (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7 || KIND == K_E2G_P7);
+  const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY ||
+                               ((KIND == K_SL_OFF || KIND == K_DL_OFF) && !S.near));
   for (int e = e0; e < e1; e++) {
     const Entry E = T.entries[e];
     const uint32_t wm = E.mask[warp];
@@ -370,16 +436,53 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
           sm[7 * kNT + i] = T.qx[s];
           sm[8 * kNT + i] = T.qy[s];
           sm[9 * kNT + i] = T.qz[s];
+          if (MIXED) {
+            sf[i] = T.fx[s];
+            sf[kNT + i] = T.fy[s];
+            sf[2 * kNT + i] = T.fz[s];
+            if (kSrcNrm) {
+              sf[3 * kNT + i] = T.fnx[s];
+              sf[4 * kNT + i] = T.fny[s];
+              sf[5 * kNT + i] = T.fnz[s];
+            }
+            sf[6 * kNT + i] = T.fa[s];
+            sf[7 * kNT + i] = T.fqx[s];
+            sf[8 * kNT + i] = T.fqy[s];
+            sf[9 * kNT + i] = T.fqz[s];
+          }
         }
         __syncthreads();
         if (wm != 0u && act) {
-          unsigned long long cr = 0, cp = 0;
-          tile_pairs<KIND>(sm, cnt, DEL, d64, S, a0, a1, a2, cr, cp);
-          if (S.near) {
+          if (all32) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+            for (int j = 0; j < cnt; j++) pair32<KIND>(sf, j, F, p0, p1, p2);
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
+            if (S.near) cplain += cnt;
+            else cfar += cnt;
+          } else if (MIXED && kPerPairSplit && S.near) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+            unsigned cr = 0;
+            for (int j = 0; j < cnt; j++) {
+              const float dx = F.px - sf[j], dy = F.py - sf[kNT + j], dz = F.pz - sf[2 * kNT + j];
+              if (dx * dx + dy * dy + dz * dz > d64f) pair32<KIND>(sf, j, F, p0, p1, p2);
+              else cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
+            }
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
             creg += cr;
-            cplain += cp - cr;
+            cplain += cnt - cr;
           } else {
-            cfar += cp;
+            unsigned cr = 0;
+            for (int j = 0; j < cnt; j++) cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
+            if (S.near) {
+              creg += cr;
+              cplain += cnt - cr;
+            } else {
+              cfar += cnt;
+            }
           }
         }
       }
@@ -388,16 +491,32 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
       const int P1 = T.P1, Pf = T.Pf, C = T.C;
       const int PT = (kSmem / C) & ~31;
       __syncthreads();
-      if (tid < 3 * P1) cheb[tid] = T.tcheb[(size_t)E.node * 3 * P1 + tid];
+      if (tid < 3 * P1) {
+        const double v = T.tcheb[(size_t)E.node * 3 * P1 + tid];
+        cheb[tid] = v;
+        if (MIXED) chebf[tid] = (float)(v - T.ctr[tid / P1]);
+      }
       const double* M = T.mom + (size_t)E.node * C * Pf;
       for (int kk0 = 0; kk0 < Pf; kk0 += PT) {
         const int cnt = min(PT, Pf - kk0);
         __syncthreads();
         for (int c = 0; c < C; c++)
-          for (int i = tid; i < cnt; i += kTB) sm[c * PT + i] = M[(size_t)c * Pf + kk0 + i];
+          for (int i = tid; i < cnt; i += kTB) {
+            const double v = M[(size_t)c * Pf + kk0 + i];
+            if (MIXED) sf[c * PT + i] = (float)v;
+            else sm[c * PT + i] = v;
+          }
         __syncthreads();
         if (wm != 0u && act) {
-          tile_proxies<DL>(sm, PT, cnt, kk0, P1, cheb, S, a0, a1, a2);
+          if (MIXED) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+            proxies32<DL>(sf, PT, cnt, kk0, P1, chebf, F, p0, p1, p2);
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
+          } else {
+            proxies64<DL>(sm, PT, cnt, kk0, P1, cheb, S, a0, a1, a2);
+          }
           cprox += cnt;
         }
       }
@@ -455,28 +574,30 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
   }
 }
 
-template <int FAM>
+template <int FAM, bool MIXED>
 __global__ void __launch_bounds__(kTB) eval_kernel(const EvalTask* __restrict__ tasks,
                                                    const BlockRef* __restrict__ blocks) {
   __shared__ double sm[kSmem];
+  __shared__ float sf[MIXED ? kSmem : 1];
   __shared__ double cheb[3 * kMaxP1];
+  __shared__ float chebf[3 * kMaxP1];
   __shared__ EvalTask sT;
   const BlockRef br = blocks[blockIdx.x];
   if (threadIdx.x == 0) sT = tasks[br.task];
   __syncthreads();
   const int kind = sT.kind;
   if (FAM == F_SL) {
-    if (kind == K_SL_ON) run_block<K_SL_ON>(sT, br.blk, sm, cheb);
-    else run_block<K_SL_OFF>(sT, br.blk, sm, cheb);
+    if (kind == K_SL_ON) run_block<K_SL_ON, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
+    else run_block<K_SL_OFF, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
   } else if (FAM == F_DL) {
-    if (kind == K_DL_ON) run_block<K_DL_ON>(sT, br.blk, sm, cheb);
-    else run_block<K_DL_OFF>(sT, br.blk, sm, cheb);
+    if (kind == K_DL_ON) run_block<K_DL_ON, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
+    else run_block<K_DL_OFF, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
   } else {
     switch (kind) {
-      case K_E2G_SL_AWAY: run_block<K_E2G_SL_AWAY>(sT, br.blk, sm, cheb); break;
-      case K_E2G_P_AWAY: run_block<K_E2G_P_AWAY>(sT, br.blk, sm, cheb); break;
-      case K_E2G_SL7: run_block<K_E2G_SL7>(sT, br.blk, sm, cheb); break;
-      default: run_block<K_E2G_P7>(sT, br.blk, sm, cheb); break;
+      case K_E2G_SL_AWAY: run_block<K_E2G_SL_AWAY, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
+      case K_E2G_P_AWAY: run_block<K_E2G_P_AWAY, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
+      case K_E2G_SL7: run_block<K_E2G_SL7, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
+      default: run_block<K_E2G_P7, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
     }
   }
 }
@@ -484,11 +605,17 @@ __global__ void __launch_bounds__(kTB) eval_kernel(const EvalTask* __restrict__ 
 }  // namespace
 
 void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_blocks, int nblocks,
-                 cudaStream_t st) {
+                 cudaStream_t st, bool mixed) {
   if (nblocks <= 0) return;
-  if (family == F_SL) eval_kernel<F_SL><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-  else if (family == F_DL) eval_kernel<F_DL><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-  else eval_kernel<F_E2G><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+  if (!mixed) {
+    if (family == F_SL) eval_kernel<F_SL, false><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+    else if (family == F_DL) eval_kernel<F_DL, false><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+    else eval_kernel<F_E2G, false><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+  } else {
+    if (family == F_SL) eval_kernel<F_SL, true><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+    else if (family == F_DL) eval_kernel<F_DL, true><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+    else eval_kernel<F_E2G, true><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+  }
 }
 
 }  // namespace hr

@@ -1,14 +1,18 @@
 // hr_pairs.cuh — per-pair regularized kernels (device functions).
 //
-// FP64 versions follow the reference formulas term by term:
+// The formulas are the reference's:
 //   reg_coeff         get_reg_coeff_7ord + evaluate_In_024   2S/utilities.cpp:163-175, 327-337
 //   sl_7ord           Stokes_SL_7ord                         2S/utilities.cpp:179-207
 //   sl_7ord_onsurf    Stokes_SL_7ord_onSurf                  2S/utilities.cpp:211-254
 //   dl_7ord           Stokes_DL_7ord                         2S/utilities.cpp:258-288
 //   dl_7ord_onsurf    Stokes_DL_7ord_onSurf                  2S/utilities.cpp:292-323
 //   lapl_dl_7ord      Lapl_DL_7ord                           E2G/utilities.cpp:190-211
-// erf, erfc, exp and sqrt are CUDA's own functions; nothing here re-derives them.
-// Branches: r < 1e-14 uses the limit values, r/delta > 8 the singular kernel.
+// evaluated from r^2 and one reciprocal square root per pair: every 1/r^k
+// of the reference becomes a product of rinv = rsqrt(r^2), r/delta becomes
+// r * (1/delta), and the switch r/delta > 8 becomes r^2 > 64 delta^2. Each
+// step changes a result by a few ulp at most; the branch values agree to
+// ~1e-28 relative at r = 8 delta, so the switch point does not matter.
+// erf, erfc, exp and rsqrt are CUDA's own functions.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -20,6 +24,20 @@ __device__ __forceinline__ double d_rootpi() { return 1.7724538509055159; }
 struct Coef {
   double c1, c2, c3;
 };
+
+// Per-target constants of the regularized kernels.
+struct Reg {
+  double d, inv_d, d64, r0sq;  // delta, 1/delta, 64 delta^2, (1e-14)^2
+};
+
+__device__ __forceinline__ Reg make_reg(double d) {
+  Reg g;
+  g.d = d;
+  g.inv_d = 1.0 / d;
+  g.d64 = 64.0 * d * d;
+  g.r0sq = 1e-28;
+  return g;
+}
 
 __device__ __forceinline__ Coef reg_coeff(double lam) {
   const double rp = d_rootpi();
@@ -38,124 +56,143 @@ __device__ __forceinline__ Coef reg_coeff(double lam) {
   return c;
 }
 
-// Regularized Stokeslet factors (s1, s2) for an off-surface target.
-__device__ __forceinline__ void sl_7ord(double r, double d, const Coef& c, double& s1, double& s2) {
+// Regularized Stokeslet factors (s1 ~ 1/r, s2 ~ 1/r^3), off-surface target.
+// Returns true when the smoothed (erf) branch was taken.
+__device__ __forceinline__ bool sl_7ord(double r2, double rinv, const Reg& g, const Coef& c,
+                                        double& s1, double& s2) {
   const double rp = d_rootpi();
-  if (r < 1e-14) {
-    s1 = 32.0 / 5.0 / rp / d;
-    s2 = 256.0 / 15.0 / rp / (d * d * d);
-  } else if (r / d > 8.0) {
-    double r2 = r * r;
-    s1 = 1.0 / r;
-    s2 = 1.0 / (r2 * r);
-  } else {
-    double rd = r / d;
-    double rd2 = rd * rd;
-    double rd4 = rd2 * rd2;
-    double rd6 = rd4 * rd2;
-    double errfn = erf(rd);
-    double r_expfn = rd * exp(-rd2);
-    double poly1 = c.c1 - 2.0 * (c.c2 + c.c3) * rd2 + 4.0 * c.c3 * rd4;
-    double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
-                   4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd6;
-    double r2 = r * r;
-    s1 = (errfn + poly1 * r_expfn) / r;
-    s2 = (errfn + poly2 * r_expfn) / (r2 * r);
+  if (r2 < g.r0sq) {
+    s1 = 32.0 / 5.0 / rp / g.d;
+    s2 = 256.0 / 15.0 / rp / (g.d * g.d * g.d);
+    return false;
   }
+  double rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s1 = rinv;
+    s2 = rinv3;
+    return false;
+  }
+  double rd = r2 * rinv * g.inv_d;
+  double rd2 = rd * rd;
+  double rd4 = rd2 * rd2;
+  double rd6 = rd4 * rd2;
+  double errfn = erf(rd);
+  double r_expfn = rd * exp(-rd2);
+  double poly1 = c.c1 - 2.0 * (c.c2 + c.c3) * rd2 + 4.0 * c.c3 * rd4;
+  double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
+                 4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd6;
+  s1 = (errfn + poly1 * r_expfn) * rinv;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  return true;
 }
 
-// Regularized Stokeslet factors for an on-surface target (lambda = 0).
-__device__ __forceinline__ void sl_7ord_onsurf(double r, double d, double& s1, double& s2) {
+// Regularized Stokeslet factors, on-surface target (lambda = 0).
+__device__ __forceinline__ bool sl_7ord_onsurf(double r2, double rinv, const Reg& g, double& s1,
+                                               double& s2) {
   const double rp = d_rootpi();
-  if (r < 1e-14) {
-    s1 = 32.0 / 5.0 / rp / d;
-    s2 = 256.0 / 15.0 / rp / (d * d * d);
-  } else if (r / d > 8.0) {
-    double r2 = r * r;
-    s1 = 1.0 / r;
-    s2 = 1.0 / (r2 * r);
-  } else {
-    double rd = r / d;
-    double rd2 = rd * rd;
-    double rd4 = rd2 * rd2;
-    double rd6 = rd4 * rd2;
-    double errfn = erf(rd);
-    double r_expfn = 2.0 / rp * rd * exp(-rd2);
-    double poly1 = 11.0 / 5.0 - 26.0 / 15.0 * rd2 + 4.0 / 15.0 * rd4;
-    double poly2 = -1.0 + (118.0 * rd2 - 68.0 * rd4 + 8.0 * rd6) / 15.0;
-    double r2 = r * r;
-    s1 = (errfn + poly1 * r_expfn) / r;
-    s2 = (errfn + poly2 * r_expfn) / (r2 * r);
+  if (r2 < g.r0sq) {
+    s1 = 32.0 / 5.0 / rp / g.d;
+    s2 = 256.0 / 15.0 / rp / (g.d * g.d * g.d);
+    return false;
   }
+  double rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s1 = rinv;
+    s2 = rinv3;
+    return false;
+  }
+  double rd = r2 * rinv * g.inv_d;
+  double rd2 = rd * rd;
+  double rd4 = rd2 * rd2;
+  double rd6 = rd4 * rd2;
+  double errfn = erf(rd);
+  double r_expfn = 2.0 / rp * rd * exp(-rd2);
+  double poly1 = 11.0 / 5.0 - 26.0 / 15.0 * rd2 + 4.0 / 15.0 * rd4;
+  double poly2 = -1.0 + (118.0 * rd2 - 68.0 * rd4 + 8.0 * rd6) * (1.0 / 15.0);
+  s1 = (errfn + poly1 * r_expfn) * rinv;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  return true;
 }
 
-// Regularized stresslet factors (s2, s3) for an off-surface target.
-__device__ __forceinline__ void dl_7ord(double r, double d, const Coef& c, double& s2, double& s3) {
+// Regularized stresslet factors (s2 ~ 1/r^3, s3 ~ 1/r^5), off-surface target.
+__device__ __forceinline__ bool dl_7ord(double r2, double rinv, const Reg& g, const Coef& c,
+                                        double& s2, double& s3) {
   const double rp = d_rootpi();
-  if (r < 1e-14) {
-    s2 = 256.0 / 15.0 / rp / (d * d * d);
+  if (r2 < g.r0sq) {
+    s2 = 256.0 / 15.0 / rp / (g.d * g.d * g.d);
     s3 = 0.0;
-  } else if (r / d > 8.0) {
-    double r2 = r * r;
-    s2 = 1.0 / (r2 * r);
-    s3 = 1.0 / (r2 * r2 * r);
-  } else {
-    double rd = r / d;
-    double rd2 = rd * rd;
-    double rd4 = rd2 * rd2;
-    double rd6 = rd4 * rd2;
-    double errfn = erf(rd);
-    double r_expfn = rd * exp(-rd2);
-    double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
-                   4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd6;
-    double poly3 = -2.0 / rp * (1.0 + 2.0 / 3.0 * rd2) +
-                   4.0 / 3.0 *
-                       ((c.c1 + 4.0 * c.c2 + 12.0 * c.c3) * rd4 - 2.0 * (c.c2 + 9.0 * c.c3) * rd6 +
-                        4.0 * c.c3 * rd6 * rd2);
-    double r2 = r * r;
-    s2 = (errfn + poly2 * r_expfn) / (r2 * r);
-    s3 = (errfn + poly3 * r_expfn) / (r2 * r2 * r);
+    return false;
   }
+  double rinv2 = rinv * rinv;
+  double rinv3 = rinv2 * rinv;
+  if (r2 > g.d64) {
+    s2 = rinv3;
+    s3 = rinv3 * rinv2;
+    return false;
+  }
+  double rd = r2 * rinv * g.inv_d;
+  double rd2 = rd * rd;
+  double rd4 = rd2 * rd2;
+  double rd6 = rd4 * rd2;
+  double errfn = erf(rd);
+  double r_expfn = rd * exp(-rd2);
+  double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
+                 4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd6;
+  double poly3 = -2.0 / rp * (1.0 + 2.0 / 3.0 * rd2) +
+                 4.0 / 3.0 *
+                     ((c.c1 + 4.0 * c.c2 + 12.0 * c.c3) * rd4 - 2.0 * (c.c2 + 9.0 * c.c3) * rd6 +
+                      4.0 * c.c3 * rd6 * rd2);
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  s3 = (errfn + poly3 * r_expfn) * (rinv3 * rinv2);
+  return true;
 }
 
-// Regularized stresslet factor s3 for an on-surface target.
-__device__ __forceinline__ double dl_7ord_onsurf(double r, double d) {
+// Regularized stresslet factor s3 ~ 1/r^5, on-surface target.
+__device__ __forceinline__ bool dl_7ord_onsurf(double r2, double rinv, const Reg& g, double& s3) {
   const double rp = d_rootpi();
-  if (r < 1e-14) {
-    return 128.0 / 45.0 / rp / (d * d * d * d * d);
-  } else if (r / d > 8.0) {
-    double r2 = r * r;
-    return 1.0 / (r2 * r2 * r);
-  } else {
-    double rd = r / d;
-    double rd2 = rd * rd;
-    double rd4 = rd2 * rd2;
-    double rd6 = rd4 * rd2;
-    double errfn = erf(rd);
-    double r_expfn = 2.0 / rp * rd * exp(-rd2);
-    double poly3 = -1.0 - 2.0 / 3.0 * rd2 + 52.0 / 45.0 * rd4 - 8.0 / 45.0 * rd6;
-    double r2 = r * r;
-    return (errfn + poly3 * r_expfn) / (r2 * r2 * r);
+  if (r2 < g.r0sq) {
+    s3 = 128.0 / 45.0 / rp / (g.d * g.d * g.d * g.d * g.d);
+    return false;
   }
+  double rinv2 = rinv * rinv;
+  double rinv5 = rinv2 * rinv2 * rinv;
+  if (r2 > g.d64) {
+    s3 = rinv5;
+    return false;
+  }
+  double rd = r2 * rinv * g.inv_d;
+  double rd2 = rd * rd;
+  double rd4 = rd2 * rd2;
+  double rd6 = rd4 * rd2;
+  double errfn = erf(rd);
+  double r_expfn = 2.0 / rp * rd * exp(-rd2);
+  double poly3 = -1.0 - 2.0 / 3.0 * rd2 + 52.0 / 45.0 * rd4 - 8.0 / 45.0 * rd6;
+  s3 = (errfn + poly3 * r_expfn) * rinv5;
+  return true;
 }
 
 // Regularized 1/r^3 kernel of the pressure (Laplace double layer type).
-__device__ __forceinline__ double lapl_dl_7ord(double r, double d, const Coef& c) {
+__device__ __forceinline__ bool lapl_dl_7ord(double r2, double rinv, const Reg& g, const Coef& c,
+                                             double& s2) {
   const double rp = d_rootpi();
-  if (r < 1e-14) {
-    return 256.0 / 15.0 / rp / (d * d * d);
-  } else if (r / d > 8.0) {
-    return 1.0 / (r * r * r);
-  } else {
-    double rd = r / d;
-    double rd2 = rd * rd;
-    double rd4 = rd2 * rd2;
-    double errfn = erf(rd);
-    double r_expfn = rd * exp(-rd2);
-    double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
-                   4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd4 * rd2;
-    return (errfn + poly2 * r_expfn) / (r * r * r);
+  if (r2 < g.r0sq) {
+    s2 = 256.0 / 15.0 / rp / (g.d * g.d * g.d);
+    return false;
   }
+  double rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s2 = rinv3;
+    return false;
+  }
+  double rd = r2 * rinv * g.inv_d;
+  double rd2 = rd * rd;
+  double rd4 = rd2 * rd2;
+  double errfn = erf(rd);
+  double r_expfn = rd * exp(-rd2);
+  double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
+                 4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd4 * rd2;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  return true;
 }
 
 }  // namespace hr

@@ -42,6 +42,29 @@ void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direc
   qx.alloc(n);
   qy.alloc(n);
   qz.alloc(n);
+  for (int k = 0; k < 3; k++) ctr[k] = S.center[k];
+  {
+    std::vector<float> a0(n), a1(n), a2(n), b0(n), b1(n), b2(n), c0(n);
+    for (int p = 0; p < n; p++) {
+      a0[p] = (float)(hx[p] - ctr[0]);
+      a1[p] = (float)(hy[p] - ctr[1]);
+      a2[p] = (float)(hz[p] - ctr[2]);
+      b0[p] = (float)hnx[p];
+      b1[p] = (float)hny[p];
+      b2[p] = (float)hnz[p];
+      c0[p] = (float)ha[p];
+    }
+    fx.upload(a0, st);
+    fy.upload(a1, st);
+    fz.upload(a2, st);
+    fnx.upload(b0, st);
+    fny.upload(b1, st);
+    fnz.upload(b2, st);
+    fa.upload(c0, st);
+    fqx.alloc(n);
+    fqy.alloc(n);
+    fqz.alloc(n);
+  }
   // upward-pass items: every non-root node (the root's moments stay zero, as
   // in the reference, which skips it: 2S/KITC.cpp:1446), in chunks of sources.
   std::vector<MomItem> it;
@@ -71,7 +94,7 @@ void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direc
 }
 
 void DevTree::set_density(Ctx& C, const double* q3_dev, bool dl, bool moments) {
-  launch_permute(n, perm.p, q3_dev, qx.p, qy.p, qz.p, C.stream);
+  launch_permute(n, perm.p, q3_dev, qx.p, qy.p, qz.p, fqx.p, fqy.p, fqz.p, C.stream);
   C.launches++;
   if (moments && nitems > 0) {
     launch_moments(dl ? 1 : 0, items.p, nitems, P1, tcheb.p, x.p, y.p, z.p, nx.p, ny.p, nz.p, a.p,
@@ -119,6 +142,17 @@ EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const D
   k.qx = T.qx.p;
   k.qy = T.qy.p;
   k.qz = T.qz.p;
+  for (int c = 0; c < 3; c++) k.ctr[c] = T.ctr[c];
+  k.fx = T.fx.p;
+  k.fy = T.fy.p;
+  k.fz = T.fz.p;
+  k.fnx = T.fnx.p;
+  k.fny = T.fny.p;
+  k.fnz = T.fnz.p;
+  k.fa = T.fa.p;
+  k.fqx = T.fqx.p;
+  k.fqy = T.fqy.p;
+  k.fqz = T.fqz.p;
   k.node_m0 = T.m0.p;
   k.node_m1 = T.m1.p;
   k.tcheb = T.tcheb.p;
@@ -159,7 +193,7 @@ void Batch::finalize(cudaStream_t st) {
 }
 
 void Batch::launch(Ctx& C) {
-  launch_eval(family, d_tasks.p, d_blocks.p, nblocks, C.stream);
+  launch_eval(family, d_tasks.p, d_blocks.p, nblocks, C.stream, !tasks.empty() && tasks[0].mixed);
   C.launches++;
 }
 

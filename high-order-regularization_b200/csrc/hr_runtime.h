@@ -91,6 +91,8 @@ struct DevTree {
   DBuf<int> perm, m0, m1;
   DBuf<double> tcheb;
   DBuf<double> qx, qy, qz;
+  DBuf<float> fx, fy, fz, fnx, fny, fnz, fa, fqx, fqy, fqz;  // FP32 copies, centre-relative
+  double ctr[3] = {0, 0, 0};
   DBuf<double> mom;  // nn * 12 * Pf
   DBuf<MomItem> items;
   DBuf<int> item_start;

@@ -1,0 +1,64 @@
+"""Mixed precision (FP32 far field with FP64 per-target accumulation, FP64
+near-surface pairs): error against the FP64 path and the relaxed GMRES.
+
+Tolerances: a mixed operator application is within 1e-6 (max-norm, relative)
+of the FP64 one; a mixed solve reaches the same 1e-10 relative residual,
+checked with an FP64 operator, and its solution agrees with the FP64
+solution to 1e-8."""
+import numpy as np
+import pytest
+import torch
+
+import highreg
+from conftest import rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def geo32():
+    return highreg.Geometry2S(32).scene
+
+
+@pytest.fixture(scope="module")
+def plan32(ctx, geo32):
+    p = highreg.Plan2S(ctx, geo32, mode=highreg.HR_TREE, P=6, N0=1000, theta=0.6)
+    yield p
+    p.close()
+
+
+def test_mixed_operator_error(plan32):
+    n = plan32.n
+    u = torch.tensor(np.random.default_rng(2).standard_normal(n), dtype=torch.float64, device="cuda")
+    y64 = torch.zeros_like(u)
+    y32 = torch.zeros_like(u)
+    plan32.matvec_dev(u, y64, highreg.HR_FP64)
+    plan32.matvec_dev(u, y32, highreg.HR_MIXED)
+    torch.cuda.synchronize()
+    e = rel_err(y32.cpu().numpy(), y64.cpu().numpy())
+    assert 0 < e < 1e-6, e
+
+
+def test_mixed_single_sums(ctx, geo32):
+    g = geo32
+    DEL = g["DEL"]
+    for mode in (highreg.HR_DIRECT, highreg.HR_TREE):
+        a = ctx.sl_offsurf(DEL, g["xq0"], g["nrm0"], g["area0"], g["f0"], g["xq1"], g["b1"], g["n01"], g["f01"],
+                           ctr=g["ctr0"], mode=mode, P=6, N0=1000)
+        b = ctx.sl_offsurf(DEL, g["xq0"], g["nrm0"], g["area0"], g["f0"], g["xq1"], g["b1"], g["n01"], g["f01"],
+                           ctr=g["ctr0"], mode=mode, P=6, N0=1000, precision=highreg.HR_MIXED)
+        assert rel_err(b, a) < 1e-6
+        a = ctx.dl_onsurf(DEL, g["xq1"], g["nrm1"], g["area1"], g["f1"], ctr=g["ctr1"], mode=mode, P=6, N0=1000)
+        b = ctx.dl_onsurf(DEL, g["xq1"], g["nrm1"], g["area1"], g["f1"], ctr=g["ctr1"], mode=mode, P=6, N0=1000,
+                          precision=highreg.HR_MIXED)
+        assert rel_err(b, a) < 1e-6
+
+
+def test_mixed_solve_reaches_fp64_residual(plan32, geo32):
+    b = plan32.rhs(geo32["f0"], geo32["f1"])
+    x64, r64 = plan32.solve(b, restart=50, tol=1e-10, true_residual=True)
+    x32, r32 = plan32.solve(b, restart=50, tol=1e-10, precision=highreg.HR_MIXED)
+    assert r32["matvecs_mixed"] > 0
+    assert r32["true_residual"] <= 1e-9
+    assert r64["true_residual"] <= 1e-9
+    assert rel_err(x32, x64) < 1e-8
