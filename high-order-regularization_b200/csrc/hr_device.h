@@ -39,18 +39,34 @@ struct EvalTask {
   const Entry* entries;                               // interaction entries
   const int* blk_start;                               // per target block, into entries
   unsigned long long* counters;  // [0] regularized pairs [1] near-target plain [2] far-target [3] proxy
+  const int* item_start;  // per target block: its work items' partial slots [start, end)
+  double* partial;        // 3 x 128 doubles per work item
 };
 
+// A piece of one entry: a near entry's source sub-range [s0, s1), or a whole
+// far entry (proxy points).
+struct Seg {
+  int entry;
+  int s0, s1;
+};
+
+// One CTA's work: a run of consecutive segments of one target block. Each
+// item writes its partial sums into its own slot; the reduce kernel adds the
+// slots of a block in order, so results do not depend on scheduling.
 struct BlockRef {
   int task;
   int blk;
+  int seg0, seg1;
+  int slot;
 };
 
 enum Family : int { F_SL = 0, F_DL = 1, F_E2G = 2 };
 
-// Evaluates every block of a combined block list in one launch.
-void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_blocks, int nblocks,
-                 cudaStream_t st, bool mixed);
+// Evaluates every work item of a combined list in one launch, then reduces
+// the partial sums per target (deterministic order) and applies the epilogue.
+void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs,
+                 int nitems, int ntask_blocks, const int2* d_task_blocks, cudaStream_t st,
+                 bool mixed);
 
 // Upward pass: proxy moments of every non-root node of a tree.
 struct MomItem {

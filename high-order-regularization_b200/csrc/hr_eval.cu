@@ -393,9 +393,11 @@ __device__ __forceinline__ void proxies32(const float* __restrict__ sf, int PT, 
 }
 
 template <int KIND, bool MIXED>
-__device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm, float* sf,
-                                          double* cheb, float* chebf) {
+__device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
+                                         const Seg* __restrict__ segs, double* sm, float* sf,
+                                         double* cheb, float* chebf) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int blk = it.blk;
   const int k = blk * kTB + tid;
   const bool valid = k < T.nt;
   const int t = valid ? T.tord[k] : 0;
@@ -406,19 +408,19 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
   const float d64f = (float)g.d64;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   unsigned long long creg = 0, cplain = 0, cfar = 0, cprox = 0;
-  const int e0 = T.blk_start[blk], e1 = T.blk_start[blk + 1];
   constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY);
   // which path a target takes through a source tile
   constexpr bool kPerPairSplit =
       (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7 || KIND == K_E2G_P7);
   const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY ||
                                ((KIND == K_SL_OFF || KIND == K_DL_OFF) && !S.near));
-  for (int e = e0; e < e1; e++) {
-    const Entry E = T.entries[e];
+  for (int q = it.seg0; q < it.seg1; q++) {
+    const Seg sg = segs[q];
+    const Entry E = T.entries[sg.entry];
     const uint32_t wm = E.mask[warp];
     const bool act = valid && ((wm >> lane) & 1u);
     if (E.type == 1) {
-      const int m0 = T.node_m0[E.node], m1 = T.node_m1[E.node];
+      const int m0 = sg.s0, m1 = sg.s1 - 1;
       for (int s0 = m0; s0 <= m1; s0 += kNT) {
         const int cnt = min(kNT, m1 - s0 + 1);
         __syncthreads();
@@ -454,28 +456,35 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
         __syncthreads();
         if (wm != 0u && act) {
           if (all32) {
-            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-            for (int j = 0; j < cnt; j++) pair32<KIND>(sf, j, F, p0, p1, p2);
-            a0 += (double)p0;
-            a1 += (double)p1;
-            a2 += (double)p2;
+            for (int j0 = 0; j0 < cnt; j0 += 16) {
+              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+              const int j1 = min(cnt, j0 + 16);
+              for (int j = j0; j < j1; j++) pair32<KIND>(sf, j, F, p0, p1, p2);
+              a0 += (double)p0;
+              a1 += (double)p1;
+              a2 += (double)p2;
+            }
             if (S.near) cplain += cnt;
             else cfar += cnt;
           } else if (MIXED && kPerPairSplit && S.near) {
-            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
             unsigned cr = 0;
-            for (int j = 0; j < cnt; j++) {
-              const float dx = F.px - sf[j], dy = F.py - sf[kNT + j], dz = F.pz - sf[2 * kNT + j];
-              if (dx * dx + dy * dy + dz * dz > d64f) pair32<KIND>(sf, j, F, p0, p1, p2);
-              else cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
+            for (int j0 = 0; j0 < cnt; j0 += 16) {
+              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+              const int j1 = min(cnt, j0 + 16);
+              for (int j = j0; j < j1; j++) {
+                const float dx = F.px - sf[j], dy = F.py - sf[kNT + j], dz = F.pz - sf[2 * kNT + j];
+                if (dx * dx + dy * dy + dz * dz > d64f) pair32<KIND>(sf, j, F, p0, p1, p2);
+                else cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
+              }
+              a0 += (double)p0;
+              a1 += (double)p1;
+              a2 += (double)p2;
             }
-            a0 += (double)p0;
-            a1 += (double)p1;
-            a2 += (double)p2;
             creg += cr;
             cplain += cnt - cr;
           } else {
             unsigned cr = 0;
+#pragma unroll 2
             for (int j = 0; j < cnt; j++) cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
             if (S.near) {
               creg += cr;
@@ -509,11 +518,13 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
         __syncthreads();
         if (wm != 0u && act) {
           if (MIXED) {
-            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-            proxies32<DL>(sf, PT, cnt, kk0, P1, chebf, F, p0, p1, p2);
-            a0 += (double)p0;
-            a1 += (double)p1;
-            a2 += (double)p2;
+            for (int i0 = 0; i0 < cnt; i0 += 16) {
+              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+              proxies32<DL>(sf + i0, PT, min(16, cnt - i0), kk0 + i0, P1, chebf, F, p0, p1, p2);
+              a0 += (double)p0;
+              a1 += (double)p1;
+              a2 += (double)p2;
+            }
           } else {
             proxies64<DL>(sm, PT, cnt, kk0, P1, cheb, S, a0, a1, a2);
           }
@@ -522,41 +533,11 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
       }
     }
   }
-  // Per-target epilogue.
-  if (valid) {
-    const double sc = T.scale;
-    double* o = T.out;
-    if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL_AWAY || KIND == K_E2G_SL7) {
-      o[3 * t] = a0 * sc;
-      o[3 * t + 1] = a1 * sc;
-      o[3 * t + 2] = a2 * sc;
-    } else if (KIND == K_DL_ON) {
-      // DL[3i+k] = u[k] * EightPI6 + 0.5 * g0[k]   (2S/KITC.cpp:1693, 2S/stresslets.cpp:271-278)
-      o[3 * t] = a0 * sc + 0.5 * S.g0[0];
-      o[3 * t + 1] = a1 * sc + 0.5 * S.g0[1];
-      o[3 * t + 2] = a2 * sc + 0.5 * S.g0[2];
-    } else if (KIND == K_DL_OFF) {
-      double xi = 0.0;
-      if (T.jump_mode == 0) {
-        // tree: xi = 1/2 on the surface, 1 inside (2S/KITC.cpp:1805-1815)
-        if (fabs(S.b) < 1.0e-12) xi = 0.5;
-        else if (S.b < 0.0) xi = 1.0;
-      } else {
-        // direct: + g0 inside or on the surface, near targets only (2S/stresslets.cpp:174-178)
-        if (S.near && ((S.b < 0.0) || (fabs(S.b) < 1.0e-14))) xi = 1.0;
-      }
-      o[3 * t] = a0 * sc + xi * S.g0[0];
-      o[3 * t + 1] = a1 * sc + xi * S.g0[1];
-      o[3 * t + 2] = a2 * sc + xi * S.g0[2];
-    } else if (KIND == K_E2G_P_AWAY) {
-      o[t] = a0 * sc;
-    } else if (KIND == K_E2G_P7) {
-      // p *= -denom_FourPI; inside: p -= f0.n0 (E2G/stokes.cpp:196-200)
-      double p = a0 * sc;
-      if (S.b < -1.e-12) p -= S.f0n0;
-      o[t] = p;
-    }
-  }
+  // partial sums of this item
+  double* o = T.partial + ((size_t)it.slot * kTB + tid) * 3;
+  o[0] = a0;
+  o[1] = a1;
+  o[2] = a2;
   // Work counters (pair kinds actually evaluated), one atomic per warp.
   if (T.counters) {
     for (int off = 16; off > 0; off >>= 1) {
@@ -575,47 +556,111 @@ __device__ __forceinline__ void run_block(const EvalTask& T, int blk, double* sm
 }
 
 template <int FAM, bool MIXED>
-__global__ void __launch_bounds__(kTB) eval_kernel(const EvalTask* __restrict__ tasks,
-                                                   const BlockRef* __restrict__ blocks) {
+__global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict__ tasks,
+                                                      const BlockRef* __restrict__ items,
+                                                      const Seg* __restrict__ segs) {
   __shared__ double sm[kSmem];
   __shared__ float sf[MIXED ? kSmem : 1];
   __shared__ double cheb[3 * kMaxP1];
   __shared__ float chebf[3 * kMaxP1];
   __shared__ EvalTask sT;
-  const BlockRef br = blocks[blockIdx.x];
-  if (threadIdx.x == 0) sT = tasks[br.task];
+  const BlockRef it = items[blockIdx.x];
+  if (threadIdx.x == 0) sT = tasks[it.task];
   __syncthreads();
   const int kind = sT.kind;
   if (FAM == F_SL) {
-    if (kind == K_SL_ON) run_block<K_SL_ON, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
-    else run_block<K_SL_OFF, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
+    if (kind == K_SL_ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
+    else run_item<K_SL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
   } else if (FAM == F_DL) {
-    if (kind == K_DL_ON) run_block<K_DL_ON, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
-    else run_block<K_DL_OFF, MIXED>(sT, br.blk, sm, sf, cheb, chebf);
+    if (kind == K_DL_ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
+    else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
   } else {
     switch (kind) {
-      case K_E2G_SL_AWAY: run_block<K_E2G_SL_AWAY, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
-      case K_E2G_P_AWAY: run_block<K_E2G_P_AWAY, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
-      case K_E2G_SL7: run_block<K_E2G_SL7, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
-      default: run_block<K_E2G_P7, MIXED>(sT, br.blk, sm, sf, cheb, chebf); break;
+      case K_E2G_SL_AWAY: run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
+      case K_E2G_P_AWAY: run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
+      case K_E2G_SL7: run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
+      default: run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
     }
+  }
+}
+
+// Sums a target block's item partials in slot order and applies the
+// reference drivers' per-target epilogue (scale and jump terms).
+__global__ void __launch_bounds__(kTB) reduce_kernel(const EvalTask* __restrict__ tasks,
+                                                     const int2* __restrict__ task_blocks) {
+  const int2 tb = task_blocks[blockIdx.x];  // (task, block)
+  const EvalTask& T = tasks[tb.x];
+  const int blk = tb.y, tid = threadIdx.x;
+  const int k = blk * kTB + tid;
+  if (k >= T.nt) return;
+  const int t = T.tord[k];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  const int s0 = T.item_start[blk], s1 = T.item_start[blk + 1];
+  for (int s = s0; s < s1; s++) {
+    const double* p = T.partial + ((size_t)s * kTB + tid) * 3;
+    a0 += p[0];
+    a1 += p[1];
+    a2 += p[2];
+  }
+  const double sc = T.scale;
+  double* o = T.out;
+  const int kind = T.kind;
+  if (kind == K_SL_ON || kind == K_SL_OFF || kind == K_E2G_SL_AWAY || kind == K_E2G_SL7) {
+    o[3 * t] = a0 * sc;
+    o[3 * t + 1] = a1 * sc;
+    o[3 * t + 2] = a2 * sc;
+  } else if (kind == K_DL_ON) {
+    // DL[3i+k] = u[k] * EightPI6 + 0.5 * g0[k]   (2S/KITC.cpp:1693, 2S/stresslets.cpp:271-278)
+    const double* g0 = T.tq + 3 * t;
+    o[3 * t] = a0 * sc + 0.5 * g0[0];
+    o[3 * t + 1] = a1 * sc + 0.5 * g0[1];
+    o[3 * t + 2] = a2 * sc + 0.5 * g0[2];
+  } else if (kind == K_DL_OFF) {
+    const double b = T.tb[t];
+    const double* g0 = T.tg0 + 3 * t;
+    double xi = 0.0;
+    if (T.jump_mode == 0) {
+      // tree: xi = 1/2 on the surface, 1 inside (2S/KITC.cpp:1805-1815)
+      if (fabs(b) < 1.0e-12) xi = 0.5;
+      else if (b < 0.0) xi = 1.0;
+    } else {
+      // direct: + g0 inside or on the surface, near targets only (2S/stresslets.cpp:174-178)
+      if (T.tnear[t] && ((b < 0.0) || (fabs(b) < 1.0e-14))) xi = 1.0;
+    }
+    o[3 * t] = a0 * sc + xi * g0[0];
+    o[3 * t + 1] = a1 * sc + xi * g0[1];
+    o[3 * t + 2] = a2 * sc + xi * g0[2];
+  } else if (kind == K_E2G_P_AWAY) {
+    o[t] = a0 * sc;
+  } else {
+    // p *= -denom_FourPI; inside: p -= f0.n0 (E2G/stokes.cpp:196-200)
+    double p = a0 * sc;
+    if (T.tb[t] < -1.e-12) {
+      const double* f0 = T.tf0 + 3 * t;
+      const double* n0 = T.tn0 + 3 * t;
+      p -= f0[0] * n0[0] + f0[1] * n0[1] + f0[2] * n0[2];
+    }
+    o[t] = p;
   }
 }
 
 }  // namespace
 
-void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_blocks, int nblocks,
-                 cudaStream_t st, bool mixed) {
-  if (nblocks <= 0) return;
-  if (!mixed) {
-    if (family == F_SL) eval_kernel<F_SL, false><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-    else if (family == F_DL) eval_kernel<F_DL, false><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-    else eval_kernel<F_E2G, false><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-  } else {
-    if (family == F_SL) eval_kernel<F_SL, true><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-    else if (family == F_DL) eval_kernel<F_DL, true><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
-    else eval_kernel<F_E2G, true><<<nblocks, kTB, 0, st>>>(d_tasks, d_blocks);
+void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs,
+                 int nitems, int ntask_blocks, const int2* d_task_blocks, cudaStream_t st,
+                 bool mixed) {
+  if (nitems > 0) {
+    if (!mixed) {
+      if (family == F_SL) eval_kernel<F_SL, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+      else if (family == F_DL) eval_kernel<F_DL, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+      else eval_kernel<F_E2G, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+    } else {
+      if (family == F_SL) eval_kernel<F_SL, true><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+      else if (family == F_DL) eval_kernel<F_DL, true><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+      else eval_kernel<F_E2G, true><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+    }
   }
+  if (ntask_blocks > 0) reduce_kernel<<<ntask_blocks, kTB, 0, st>>>(d_tasks, d_task_blocks);
 }
 
 }  // namespace hr

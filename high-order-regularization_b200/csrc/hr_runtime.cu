@@ -174,27 +174,107 @@ EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const D
   return k;
 }
 
-void Batch::finalize(cudaStream_t st) {
-  std::vector<std::pair<double, BlockRef>> all;
+void Batch::finalize(cudaStream_t st, int num_sms) {
+  // 1. segments: a far entry whole, a near entry cut into source ranges of
+  //    at most kSegSrc; cost ~ active warps x pair evaluations.
+  constexpr int kSegSrc = 1024;
+  struct HSeg {
+    Seg s;
+    double cost;
+  };
+  std::vector<std::vector<std::vector<HSeg>>> per(tasks.size());
+  double total = 0.0;
   for (size_t t = 0; t < tasks.size(); t++) {
     const Lists& L = *lists[t];
-    for (int b = 0; b < L.nblocks(); b++) all.push_back({L.blk_cost[b], BlockRef{(int)t, b}});
+    const Tree& T = *trees[t];
+    const int P1 = T.P + 1;
+    const double Pf = (double)P1 * P1 * P1;
+    per[t].resize(L.nblocks());
+    for (int b = 0; b < L.nblocks(); b++) {
+      for (int e = L.blk_start[b]; e < L.blk_start[b + 1]; e++) {
+        const Entry& E = L.entries[e];
+        int warps = 0;
+        for (int w = 0; w < 4; w++) warps += E.mask[w] != 0u;
+        if (E.type == 0) {
+          double c = warps * Pf * 1.5;
+          per[t][b].push_back({Seg{e, 0, 0}, c});
+          total += c;
+        } else {
+          for (int s0 = T.m0[E.node]; s0 <= T.m1[E.node]; s0 += kSegSrc) {
+            int s1 = std::min(T.m1[E.node] + 1, s0 + kSegSrc);
+            double c = warps * (double)(s1 - s0) * 2.0;
+            per[t][b].push_back({Seg{e, s0, s1}, c});
+            total += c;
+          }
+        }
+      }
+    }
   }
-  // longest first: the hardware dispatches CTAs roughly in index order
-  std::stable_sort(all.begin(), all.end(),
+  // 2. items: runs of consecutive segments of one block, each about
+  //    total / (SMs x 4 resident CTAs x 6 waves), never below four tiles.
+  const double target = std::max(total / (num_sms * 4.0 * 6.0), 4.0 * 256.0 * 2.0);
+  std::vector<Seg> segs;
+  std::vector<std::pair<double, BlockRef>> items;
+  std::vector<int> starts;
+  std::vector<size_t> start_off(tasks.size());
+  std::vector<int2> tblocks;
+  int slot = 0;
+  for (size_t t = 0; t < tasks.size(); t++) {
+    start_off[t] = starts.size();
+    const int nb = (int)per[t].size();
+    for (int b = 0; b < nb; b++) {
+      starts.push_back(slot);
+      tblocks.push_back(make_int2((int)t, b));
+      const auto& v = per[t][b];
+      size_t i = 0;
+      while (i < v.size()) {
+        BlockRef it;
+        it.task = (int)t;
+        it.blk = b;
+        it.seg0 = (int)segs.size();
+        double c = 0.0;
+        do {
+          segs.push_back(v[i].s);
+          c += v[i].cost;
+          i++;
+        } while (i < v.size() && c + v[i].cost <= target);
+        it.seg1 = (int)segs.size();
+        it.slot = slot++;
+        items.push_back({c, it});
+      }
+      if (v.empty()) {
+        // a block without work still gets one (empty) item so that its
+        // partial slot is written
+        BlockRef it{(int)t, b, (int)segs.size(), (int)segs.size(), slot++};
+        items.push_back({0.0, it});
+      }
+    }
+    starts.push_back(slot);
+  }
+  std::stable_sort(items.begin(), items.end(),
                    [](const std::pair<double, BlockRef>& a, const std::pair<double, BlockRef>& b) {
                      return a.first > b.first;
                    });
-  std::vector<BlockRef> br(all.size());
-  for (size_t i = 0; i < all.size(); i++) br[i] = all[i].second;
-  nblocks = (int)br.size();
-  d_blocks.upload(br, st);
+  std::vector<BlockRef> br(items.size());
+  for (size_t i = 0; i < items.size(); i++) br[i] = items[i].second;
+  nitems = (int)br.size();
+  ntask_blocks = (int)tblocks.size();
+  d_items.upload(br, st);
+  d_segs.upload(segs, st);
+  d_item_start.upload(starts, st);
+  d_task_blocks.upload(tblocks, st);
+  d_partial.alloc((size_t)std::max(1, slot) * kTB * 3);
+  for (size_t t = 0; t < tasks.size(); t++) {
+    tasks[t].item_start = d_item_start.p + start_off[t];
+    tasks[t].partial = d_partial.p;
+  }
   d_tasks.upload(tasks, st);
 }
 
 void Batch::launch(Ctx& C) {
-  launch_eval(family, d_tasks.p, d_blocks.p, nblocks, C.stream, !tasks.empty() && tasks[0].mixed);
-  C.launches++;
+  launch_eval(family, d_tasks.p, d_items.p, d_segs.p, nitems, ntask_blocks, d_task_blocks.p,
+              C.stream, !tasks.empty() && tasks[0].mixed);
+  C.launches += 2;
 }
 
 }  // namespace hr

@@ -79,6 +79,7 @@ struct Ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   long long launches = 0;
+  int num_sms = 148;
   DBuf<unsigned long long> counters;  // [0] reg pairs [1] plain pairs [2] proxies
 };
 
@@ -131,10 +132,16 @@ struct Batch {
   int family = F_SL;
   std::vector<EvalTask> tasks;
   std::vector<const Lists*> lists;
+  std::vector<const Tree*> trees;  // source tree of each task (member ranges of near entries)
   DBuf<EvalTask> d_tasks;
-  DBuf<BlockRef> d_blocks;
-  int nblocks = 0;
-  void finalize(cudaStream_t st);  // builds the combined cost-sorted block list
+  DBuf<BlockRef> d_items;
+  DBuf<Seg> d_segs;
+  DBuf<int> d_item_start;
+  DBuf<int2> d_task_blocks;
+  DBuf<double> d_partial;
+  int nitems = 0, ntask_blocks = 0;
+  // builds the segments and cost-balanced work items of all tasks
+  void finalize(cudaStream_t st, int num_sms = 148);
   void launch(Ctx& C);
 };
 
