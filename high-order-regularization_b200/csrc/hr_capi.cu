@@ -10,10 +10,6 @@
 
 using namespace hr;
 
-struct hr_ctx {
-  Ctx c;
-};
-
 namespace hr {
 // implemented in hr_poisson.cu
 void dst_poisson3d_dev(Ctx& C, int n, double* f_dev);

@@ -1,0 +1,330 @@
+// hr_e2g.cu — the extend-to-grid pipeline on the device
+// (test_Stokes_Poisson3d_FD, E2G/main.cpp:107-424):
+//   1. pressure and velocity boundary integrals at the six box faces with the
+//      plain kernels and at the BAND1 grid points outside or on the surface
+//      with the 7th-order regularized kernels and subtraction (one batched
+//      launch of four sums, E2G/main.cpp:1049-1406);
+//   2. p = 0 and u = (1, 0, 0) elsewhere, then the four Poisson extensions:
+//      p first (variable 0), then u_x, u_y, u_z with the extended p
+//      (E2G/main.cpp:195-200, 403-424).
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../host/hr_e2g_geom.h"
+#include "hr_runtime.h"
+
+namespace hr {
+void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const uint8_t* out_dev,
+                       const double* p_dev, double* u_dev, int variable);
+}
+
+using namespace hr;
+
+namespace {
+
+__global__ void fill_kernel(long n, double v, double* a) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) a[i] = v;
+}
+
+__global__ void scatter_kernel(int n, int comps, const long* __restrict__ gi,
+                               const double* __restrict__ v, double* g0, double* g1, double* g2) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  long g = gi[t];
+  if (comps == 1) {
+    g0[g] = v[t];
+  } else {
+    g0[g] = v[3 * t];
+    g1[g] = v[3 * t + 1];
+    g2[g] = v[3 * t + 2];
+  }
+}
+
+constexpr double kPI = 3.14159265358979323846;
+
+}  // namespace
+
+struct hr_e2g {
+  hr_ctx* owner = nullptr;
+  e2g_setup::Scene S;
+  int nface = 0, nband = 0;
+  DevTree tree;
+  DBuf<double> q3;
+  DevTargets tf, tb;
+  DevLists Lf, Lb;
+  DBuf<double> pf, uf, pb, ub;
+  DBuf<long> gf, gb;
+  DBuf<uint8_t> mband2, mout;
+  DBuf<double> p_bi, u_bi, p_ext, u_ext;  // grids
+  Batch batch[2];                         // FP64, mixed
+  long long pairs = 0;
+};
+
+extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
+  if (!ctx || !out || N < 36 || N % 2 != 0) return HR_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<hr_e2g> E(new hr_e2g);
+  E->owner = ctx;
+  Ctx& C = ctx->c;
+  try {
+    HR_CHECK_CUDA(cudaSetDevice(C.device));
+    cudaStream_t st = C.stream;
+    e2g_setup::build(E->S, N, 4.0, 2.0);  // BAND1, BAND2: E2G/main.cpp:112-113
+    const auto& S = E->S;
+    const int M = N + 1;
+    const double h = S.h;
+    // surface (direct sums: a single node holding every source)
+    hr_surface surf;
+    memset(&surf, 0, sizeof(surf));
+    surf.n = (int)S.area.size();
+    surf.xyz = S.xq.data();
+    surf.nrml = S.nrm.data();
+    surf.area = S.area.data();
+    surf.center[0] = surf.center[1] = surf.center[2] = 1.5;
+    E->tree.build(surf, 6, 1000, 0.6, true, st);
+    E->q3.upload(S.f, st);
+    E->tree.set_density(C, E->q3.p, false, false);
+    // face targets in the reference loop order (E2G/main.cpp:1058-1075)
+    std::vector<double> fx;
+    std::vector<long> fg;
+    for (int i = 0; i <= N; i++)
+      for (int j = 0; j <= N; j++)
+        for (int k = 0; k <= N; k++)
+          if (i == 0 || i == N || j == 0 || j == N || k == 0 || k == N) {
+            fx.insert(fx.end(), {i * h, j * h, k * h});
+            fg.push_back(((long)i * M + j) * M + k);
+          }
+    // band targets outside or on the surface (E2G/main.cpp:1133-1162)
+    std::vector<double> bx, bb, bx0, bn0, bf0;
+    std::vector<long> bg;
+    for (int i = 1; i < N; i++)
+      for (int j = 1; j < N; j++)
+        for (int k = 1; k < N; k++) {
+          long g = ((long)i * M + j) * M + k;
+          int ind = S.nrst[g];
+          if (ind == -1) continue;
+          double b = S.b[ind];
+          if ((b > 0.0) || (fabs(b) < 1.e-12)) {
+            bx.insert(bx.end(), {i * h, j * h, k * h});
+            bb.push_back(b);
+            const double* x0 = &S.x0[3 * ind];
+            bx0.insert(bx0.end(), {x0[0], x0[1], x0[2]});
+            bn0.insert(bn0.end(), {S.n0[3 * ind], S.n0[3 * ind + 1], S.n0[3 * ind + 2]});
+            double f0[3];
+            e2g_setup::stokeslet_density(x0, f0);
+            bf0.insert(bf0.end(), {f0[0], f0[1], f0[2]});
+            bg.push_back(g);
+          }
+        }
+    E->nface = (int)fg.size();
+    E->nband = (int)bg.size();
+    auto up = [&](DevTargets& T, int n, const std::vector<double>& x, const double* b,
+                  const double* x0, const double* n0, const double* f0) {
+      T.n = n;
+      T.xyz.upload(x.data(), 3 * (size_t)n, st);
+      if (b) T.b.upload(b, n, st);
+      else {
+        T.b.alloc(n);
+        T.b.zero(st);
+      }
+      T.x0.alloc(3 * (size_t)n);
+      if (x0) T.x0.upload(x0, 3 * (size_t)n, st);
+      T.n0.alloc(3 * (size_t)n);
+      if (n0) T.n0.upload(n0, 3 * (size_t)n, st);
+      else T.n0.zero(st);
+      T.f0.alloc(3 * (size_t)n);
+      if (f0) T.f0.upload(f0, 3 * (size_t)n, st);
+      else T.f0.zero(st);
+      T.g0.alloc(3 * (size_t)n);
+      T.nrm.alloc(3 * (size_t)n);
+      std::vector<uint8_t> nr(n, 1);
+      T.near.upload(nr, st);
+    };
+    up(E->tf, E->nface, fx, nullptr, nullptr, nullptr, nullptr);
+    up(E->tb, E->nband, bx, bb.data(), bx0.data(), bn0.data(), bf0.data());
+    E->Lf.build(E->tree.host, E->nface, fx.data(), nullptr, st);
+    E->Lb.build(E->tree.host, E->nband, bx.data(), nullptr, st);
+    E->gf.upload(fg, st);
+    E->gb.upload(bg, st);
+    E->pf.alloc(E->nface);
+    E->uf.alloc(3 * (size_t)E->nface);
+    E->pb.alloc(std::max(1, E->nband));
+    E->ub.alloc(3 * (size_t)std::max(1, E->nband));
+    const double p_scale = 1.0 / (4.0 * kPI), sl_scale = 1.0 / (8.0 * kPI);
+    for (int prec = 0; prec < 2; prec++) {
+      Batch& B = E->batch[prec];
+      B.family = F_E2G;
+      EvalTask a = make_task(K_E2G_P_AWAY, S.delta, p_scale, E->tree, E->Lf, E->tf, E->pf.p);
+      EvalTask b = make_task(K_E2G_SL_AWAY, S.delta, sl_scale, E->tree, E->Lf, E->tf, E->uf.p);
+      EvalTask c = make_task(K_E2G_P7, S.delta, -p_scale, E->tree, E->Lb, E->tb, E->pb.p);
+      EvalTask d = make_task(K_E2G_SL7, S.delta, sl_scale, E->tree, E->Lb, E->tb, E->ub.p);
+      for (EvalTask* t : {&a, &b, &c, &d}) {
+        t->mixed = prec;
+        t->jump_mode = 1;
+      }
+      B.tasks = {a, b, c, d};
+      B.lists = {&E->Lf.host, &E->Lf.host, &E->Lb.host, &E->Lb.host};
+      B.trees = {&E->tree.host, &E->tree.host, &E->tree.host, &E->tree.host};
+      B.finalize(st, C.num_sms);
+    }
+    E->pairs = 2LL * (E->nface + E->nband) * (long long)surf.n;
+    // masks: BAND2 points, and exterior points outside BAND2 (E2G/main.cpp:1611-1614, 1654-1672)
+    std::vector<uint8_t> b2((size_t)M * M * M, 0), om((size_t)M * M * M, 0);
+    for (int i = 0; i < M; i++)
+      for (int j = 0; j < M; j++)
+        for (int k = 0; k < M; k++) {
+          long g = ((long)i * M + j) * M + k;
+          int ind = S.nrst[g];
+          if (ind != -1 && S.band2[ind]) b2[g] = 1;
+          double x[3] = {i * h, j * h, k * h};
+          double u0 = x[0] - 1.5, u1 = x[1] - 1.5, u2 = x[2] - 1.5;
+          double levl = u0 * u0 / 1.0 + u1 * u1 / 0.25 + u2 * u2 / 0.25 - 1.0;
+          if (levl > 0 && (ind == -1 || !S.band2[ind])) om[g] = 1;
+        }
+    E->mband2.upload(b2, st);
+    E->mout.upload(om, st);
+    size_t m3 = (size_t)M * M * M;
+    E->p_bi.alloc(m3);
+    E->u_bi.alloc(3 * m3);
+    E->p_ext.alloc(m3);
+    E->u_ext.alloc(3 * m3);
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+  } catch (const hr::Error& e) {
+    C.err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    C.err = e.what();
+    return HR_ERR_CUDA;
+  }
+  *out = E.release();
+  return HR_OK;
+}
+
+extern "C" int hr_e2g_get_info(const hr_e2g* E, hr_e2g_info* info) {
+  if (!E || !info) return HR_ERR_ARG;
+  info->N = E->S.N;
+  info->L = E->S.L;
+  info->h = E->S.h;
+  info->delta = E->S.delta;
+  info->nq = (int)E->S.area.size();
+  info->n_tagged = (int)E->S.b.size();
+  info->n_band = E->nband;
+  info->n_face = E->nface;
+  info->pairs = E->pairs;
+  return HR_OK;
+}
+
+extern "C" int hr_e2g_run(hr_e2g* E, int precision, hr_e2g_report* rep) {
+  if (!E) return HR_ERR_ARG;
+  Ctx& C = E->owner->c;
+  try {
+    HR_CHECK_CUDA(cudaSetDevice(C.device));
+    cudaStream_t st = C.stream;
+    const int N = E->S.N, M = N + 1;
+    const long m3 = (long)M * M * M;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) HR_CHECK_CUDA(cudaEventCreate(&e));
+    HR_CHECK_CUDA(cudaEventRecord(ev[0], st));
+    E->batch[precision == HR_MIXED ? 1 : 0].launch(C);
+    HR_CHECK_CUDA(cudaEventRecord(ev[1], st));
+    // grids: p = 0, u = (1, 0, 0) off the evaluated points (E2G/main.cpp:1062, 1234-1236)
+    int fb = 148 * 8;
+    fill_kernel<<<fb, 256, 0, st>>>(m3, 0.0, E->p_bi.p);
+    fill_kernel<<<fb, 256, 0, st>>>(m3, 1.0, E->u_bi.p);
+    fill_kernel<<<fb, 256, 0, st>>>(2 * m3, 0.0, E->u_bi.p + m3);
+    double *ux = E->u_bi.p, *uy = ux + m3, *uz = uy + m3;
+    scatter_kernel<<<(E->nface + 255) / 256, 256, 0, st>>>(E->nface, 1, E->gf.p, E->pf.p, E->p_bi.p,
+                                                           nullptr, nullptr);
+    scatter_kernel<<<(E->nface + 255) / 256, 256, 0, st>>>(E->nface, 3, E->gf.p, E->uf.p, ux, uy, uz);
+    if (E->nband > 0) {
+      scatter_kernel<<<(E->nband + 255) / 256, 256, 0, st>>>(E->nband, 1, E->gb.p, E->pb.p, E->p_bi.p,
+                                                             nullptr, nullptr);
+      scatter_kernel<<<(E->nband + 255) / 256, 256, 0, st>>>(E->nband, 3, E->gb.p, E->ub.p, ux, uy, uz);
+    }
+    C.launches += 7;
+    HR_CHECK_CUDA(cudaGetLastError());
+    HR_CHECK_CUDA(cudaEventRecord(ev[2], st));
+    // Poisson extensions: p (variable 0) then u_x, u_y, u_z with the extended p
+    HR_CHECK_CUDA(cudaMemcpyAsync(E->p_ext.p, E->p_bi.p, sizeof(double) * m3, cudaMemcpyDeviceToDevice, st));
+    solve_poisson_dev(C, N, E->S.L, E->mband2.p, E->mout.p, nullptr, E->p_ext.p, 0);
+    HR_CHECK_CUDA(cudaMemcpyAsync(E->u_ext.p, E->u_bi.p, sizeof(double) * 3 * m3, cudaMemcpyDeviceToDevice, st));
+    for (int v = 0; v < 3; v++)
+      solve_poisson_dev(C, N, E->S.L, E->mband2.p, E->mout.p, E->p_ext.p, E->u_ext.p + v * m3, v + 1);
+    HR_CHECK_CUDA(cudaEventRecord(ev[3], st));
+    HR_CHECK_CUDA(cudaEventSynchronize(ev[3]));
+    float t01 = 0, t23 = 0, t03 = 0;
+    cudaEventElapsedTime(&t01, ev[0], ev[1]);
+    cudaEventElapsedTime(&t23, ev[2], ev[3]);
+    cudaEventElapsedTime(&t03, ev[0], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (rep) {
+      memset(rep, 0, sizeof(*rep));
+      rep->seconds_sums = t01 * 1e-3;
+      rep->seconds_poisson = t23 * 1e-3;
+      rep->seconds_total = t03 * 1e-3;
+      rep->pairs = E->pairs;
+    }
+  } catch (const hr::Error& e) {
+    C.err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    C.err = e.what();
+    return HR_ERR_CUDA;
+  }
+  return HR_OK;
+}
+
+// which: 0 p after the sums, 1 u after the sums (3 grids), 2 extended p, 3 extended u (3 grids)
+extern "C" int hr_e2g_get(hr_e2g* E, int which, double* out) {
+  if (!E || !out || which < 0 || which > 3) return HR_ERR_ARG;
+  Ctx& C = E->owner->c;
+  try {
+    const long M = E->S.N + 1, m3 = M * M * M;
+    const double* src = which == 0 ? E->p_bi.p : which == 1 ? E->u_bi.p : which == 2 ? E->p_ext.p : E->u_ext.p;
+    long n = (which == 1 || which == 3) ? 3 * m3 : m3;
+    HR_CHECK_CUDA(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, C.stream));
+    HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
+  } catch (const hr::Error& e) {
+    C.err = e.what();
+    return e.code;
+  }
+  return HR_OK;
+}
+
+// scene data for checks: which 0 = quadrature (3nq xyz, 3nq nrml, nq area, 3nq f),
+// 1 = nrst grid (int), 2 = tagged targets (b, x0, n0, band2 as double)
+extern "C" int hr_e2g_scene(const hr_e2g* E, int which, void* out) {
+  if (!E || !out) return HR_ERR_ARG;
+  const auto& S = E->S;
+  if (which == 0) {
+    double* o = (double*)out;
+    size_t nq = S.area.size();
+    memcpy(o, S.xq.data(), 3 * nq * sizeof(double));
+    memcpy(o + 3 * nq, S.nrm.data(), 3 * nq * sizeof(double));
+    memcpy(o + 6 * nq, S.area.data(), nq * sizeof(double));
+    memcpy(o + 7 * nq, S.f.data(), 3 * nq * sizeof(double));
+  } else if (which == 1) {
+    memcpy(out, S.nrst.data(), S.nrst.size() * sizeof(int));
+  } else if (which == 2) {
+    double* o = (double*)out;
+    size_t nt = S.b.size();
+    memcpy(o, S.b.data(), nt * sizeof(double));
+    memcpy(o + nt, S.x0.data(), 3 * nt * sizeof(double));
+    memcpy(o + 4 * nt, S.n0.data(), 3 * nt * sizeof(double));
+    for (size_t t = 0; t < nt; t++) o[7 * nt + t] = S.band2[t];
+  } else {
+    return HR_ERR_ARG;
+  }
+  return HR_OK;
+}
+
+extern "C" void hr_e2g_destroy(hr_e2g* E) {
+  if (!E) return;
+  cudaStreamSynchronize(E->owner->c.stream);
+  delete E;
+}
+
+extern "C" double hr_e2g_p_exact(double x, double y, double z) { return e2g_setup::p_exact(x, y, z); }
+extern "C" void hr_e2g_u_exact(double x, double y, double z, double* u) { e2g_setup::u_exact(x, y, z, u); }

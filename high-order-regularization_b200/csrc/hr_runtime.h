@@ -149,3 +149,8 @@ EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const D
                    const DevTargets& tg, double* out);
 
 }  // namespace hr
+
+// The C ABI's opaque context.
+struct hr_ctx {
+  hr::Ctx c;
+};

@@ -454,3 +454,70 @@ class Plan2S:
         v = ctypes.c_double()
         self.ctx._check(lib().hr_plan2s_time_batch(self.p, which, iters, ctypes.byref(v)))
         return v.value
+
+
+class E2GInfo(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_int), ("L", ctypes.c_double), ("h", ctypes.c_double), ("delta", ctypes.c_double),
+                ("nq", ctypes.c_int), ("n_tagged", ctypes.c_int), ("n_band", ctypes.c_int), ("n_face", ctypes.c_int),
+                ("pairs", ctypes.c_longlong)]
+
+
+class E2GReport(ctypes.Structure):
+    _fields_ = [("seconds_sums", ctypes.c_double), ("seconds_poisson", ctypes.c_double),
+                ("seconds_total", ctypes.c_double), ("pairs", ctypes.c_longlong)]
+
+
+class E2G:
+    """The extend-to-grid pipeline (translating spheroid, h = 3/N) on the device."""
+
+    def __init__(self, ctx: Context, N: int):
+        self.ctx = ctx
+        p = ctypes.c_void_p()
+        ctx._check(lib().hr_e2g_create(ctx.p, N, ctypes.byref(p)))
+        self.p = p
+        info = E2GInfo()
+        lib().hr_e2g_get_info(p, ctypes.byref(info))
+        self.info = {k: getattr(info, k) for k, _ in E2GInfo._fields_}
+        self.N = N
+
+    def close(self):
+        if self.p:
+            lib().hr_e2g_destroy(self.p)
+            self.p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, precision=HR_FP64):
+        rep = E2GReport()
+        self.ctx._check(lib().hr_e2g_run(self.p, precision, ctypes.byref(rep)))
+        return {k: getattr(rep, k) for k, _ in E2GReport._fields_}
+
+    def get(self, which):
+        m = (self.N + 1) ** 3
+        out = np.zeros(3 * m if which in (1, 3) else m)
+        self.ctx._check(lib().hr_e2g_get(self.p, which, _dp(out)))
+        return out
+
+    def scene(self):
+        nq, nt = self.info["nq"], self.info["n_tagged"]
+        q = np.zeros(10 * nq)
+        lib().hr_e2g_scene(self.p, 0, q.ctypes.data_as(ctypes.c_void_p))
+        nrst = np.zeros((self.N + 1) ** 3, np.int32)
+        lib().hr_e2g_scene(self.p, 1, nrst.ctypes.data_as(ctypes.c_void_p))
+        t = np.zeros(8 * nt)
+        lib().hr_e2g_scene(self.p, 2, t.ctypes.data_as(ctypes.c_void_p))
+        return dict(xq=q[:3 * nq], nrm=q[3 * nq:6 * nq], area=q[6 * nq:7 * nq], f=q[7 * nq:10 * nq], nrst=nrst,
+                    b=t[:nt], x0=t[nt:4 * nt], n0=t[4 * nt:7 * nt], band2=t[7 * nt:].astype(np.int32))
+
+
+def e2g_exact(x, y, z):
+    """Exact pressure and velocity of the translating spheroid at one point."""
+    L = lib()
+    L.hr_e2g_p_exact.restype = ctypes.c_double
+    u = np.zeros(3)
+    L.hr_e2g_u_exact(ctypes.c_double(x), ctypes.c_double(y), ctypes.c_double(z), _dp(u))
+    return L.hr_e2g_p_exact(ctypes.c_double(x), ctypes.c_double(y), ctypes.c_double(z)), u

@@ -1,0 +1,357 @@
+// hr_e2g_geom.cpp — host setup of the extend-to-grid problem: the translating
+// prolate spheroid of highreg_stokes_extend_to_grid (semi-axes 1, .5, .5,
+// centre (1.5, 1.5, 1.5), box [0, 3]^3, h = 3/N):
+//   * quadrature points on grid-line crossings (Generate_Surface,
+//     E2G/surface.cpp:12-66, grid offset by the centre),
+//   * the exact surface force of the translating body (stokeslet_density,
+//     E2G/utilities.cpp:267-285) and the exact pressure and velocity
+//     (p_exact, SL_exact: E2G/utilities.cpp:294-411),
+//   * the BAND1 = 4h / BAND2 = 2h tagging of grid points with their nearest
+//     surface point and signed distance (find_nrst_surfc, E2G/surface.cpp:303-392).
+// The reference tags grid points while scanning quadrature points in order,
+// so the target numbering is "by first claiming quadrature point, then i, j,
+// k"; the same numbering is produced here with a parallel first-claim pass.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "hr_e2g_geom.h"
+
+namespace e2g_setup {
+
+constexpr double kPI = 3.14159265358979323846;
+constexpr double kCtr = 1.5;                   // E2G/utilities.h:19
+const double kAx[3] = {1.0, 0.5, 0.5};         // E2G/utilities.h:12-14
+
+inline double phi(const double* y) {
+  double x0 = y[0] - kCtr, x1 = y[1] - kCtr, x2 = y[2] - kCtr;
+  return x0 * x0 / (kAx[0] * kAx[0]) + x1 * x1 / (kAx[1] * kAx[1]) + x2 * x2 / (kAx[2] * kAx[2]) - 1.0;
+}
+inline double dphi(int i, const double* y) { return 2.0 * (y[i] - kCtr) / (kAx[i] * kAx[i]); }
+
+// stokeslet_density: E2G/utilities.cpp:267-285
+void stokeslet_density(const double* pt, double* f) {
+  double x = pt[0] - kCtr;
+  double a = kAx[0], b = kAx[1];
+  double a_sq = a * a, b_sq = b * b;
+  double x_sq = x * x;
+  double e_sq = 1.0 - b_sq / a_sq;
+  double e = sqrt(e_sq);
+  double Le = log((1.0 + e) / (1.0 - e));
+  f[0] = 4.0 * e_sq * e * a / b / ((1.0 + e_sq) * Le - 2.0 * e) / sqrt(a_sq - e_sq * x_sq);
+  f[1] = 0.0;
+  f[2] = 0.0;
+}
+
+// p_exact: E2G/utilities.cpp:294-321
+double p_exact(double xi, double yi, double zi) {
+  double x = xi - kCtr, y = yi - kCtr, z = zi - kCtr;
+  double a_sq = kAx[0] * kAx[0], b_sq = kAx[1] * kAx[1];
+  double r_sq = y * y + z * z;
+  double c = sqrt(a_sq - b_sq);
+  double R1 = sqrt((x + c) * (x + c) + r_sq);
+  double R2 = sqrt((x - c) * (x - c) + r_sq);
+  double dB1dx = 1.0 / R1 - 1.0 / R2;
+  double e = c / kAx[0];
+  double Le = log((1.0 + e) / (1.0 - e));
+  double a1 = e * e / ((1.0 + e * e) * Le - 2.0 * e);
+  return -2.0 * a1 * dB1dx;
+}
+
+// SL_exact: E2G/utilities.cpp:360-411
+void u_exact(double xi, double yi, double zi, double* u) {
+  double x = xi - kCtr, y = yi - kCtr, z = zi - kCtr;
+  double a_sq = kAx[0] * kAx[0], b_sq = kAx[1] * kAx[1];
+  double r_sq = y * y + z * z;
+  double c = sqrt(a_sq - b_sq);
+  double R1 = sqrt((x + c) * (x + c) + r_sq);
+  double R2 = sqrt((x - c) * (x - c) + r_sq);
+  double R1c = R1 - (x + c);
+  double R2c = R2 - (x - c);
+  double B10;
+  if (r_sq < 1.e-14) {
+    if (x < 0) B10 = log((x - c) / (x + c));
+    else B10 = log((x + c) / (x - c));
+  } else {
+    B10 = log(R2c / R1c);
+  }
+  double B30 = (x + c) / R1 - (x - c) / R2;
+  double dB1dx = 1.0 / R1 - 1.0 / R2;
+  double dB1dyz = 0.0;
+  if (r_sq > 1.e-14) dB1dyz = 1.0 / R2 / R2c - 1.0 / R1 / R1c;
+  double dB3dyz = 1.0 / R2 - 1.0 / R1 + x * dB1dyz;
+  double e = c / kAx[0];
+  double Le = log((1.0 + e) / (1.0 - e));
+  double a1 = e * e / ((1.0 + e * e) * Le - 2.0 * e);
+  double b1 = a1 * (1.0 - e * e) / (2.0 * e * e);
+  u[0] = 2.0 * a1 * B10 - a1 * B30 + 2.0 * b1 * ((x - c) / R2 - (x + c) / R1 + B10 + x * dB1dx);
+  double Er = a1 * (1.0 / R2 - 1.0 / R1) + 2.0 * b1 * dB3dyz;
+  u[1] = Er * y;
+  u[2] = Er * z;
+}
+
+namespace {
+constexpr double kTol = 1e-14;
+const double kTheta = 70.0 * kPI / 180.0;
+
+double bump(double r) {
+  double b = 0.0;
+  if (fabs(r) < 1.0) {
+    double r2 = r * r;
+    b = exp(2.0 * r2 / (r2 - 1.0));
+  }
+  return b;
+}
+double part_unity(int i, const double* n) {
+  double v[3] = {bump(acos(fabs(n[0])) / kTheta), bump(acos(fabs(n[1])) / kTheta),
+                 bump(acos(fabs(n[2])) / kTheta)};
+  double vs = v[0] + v[1] + v[2];
+  return v[i] / vs;
+}
+
+double bisection(const double* PT, double H, int i, double a, double b) {
+  double xl[3] = {PT[0], PT[1], PT[2]}, xr[3] = {PT[0], PT[1], PT[2]}, xm[3] = {PT[0], PT[1], PT[2]};
+  xl[i] += a * H;
+  xr[i] += b * H;
+  if (phi(xl) * phi(xr) > 0.0) return 0.0;
+  if (fabs(phi(xl)) <= kTol) return a;
+  if (fabs(phi(xr)) <= kTol) return b;
+  double p = (a + b) / 2;
+  xm[i] = PT[i] + p * H;
+  double pm = phi(xm);
+  int guard = 0;
+  while (fabs(pm) > kTol && guard++ < 2000) {
+    if (phi(xl) * phi(xm) < 0.0) b = p;
+    else {
+      a = p;
+      memcpy(xl, xm, sizeof(xl));
+    }
+    p = (a + b) / 2;
+    xm[i] = PT[i] + p * H;
+    pm = phi(xm);
+  }
+  return p;
+}
+
+// Newton: E2G/surface.cpp:88-128
+double newton(const double* PT, double H, int i, double a, double b) {
+  double xl[3] = {PT[0], PT[1], PT[2]}, xr[3] = {PT[0], PT[1], PT[2]}, xn[3] = {PT[0], PT[1], PT[2]};
+  xl[i] += a * H;
+  xr[i] += b * H;
+  int n = 0;
+  if (phi(xl) * phi(xr) > 0.0) return 0.0;
+  if (fabs(phi(xl)) <= kTol) return a;
+  if (fabs(phi(xr)) <= kTol) return b;
+  double p = (a + b) / 2;
+  xn[i] = PT[i] + p * H;
+  double ph = phi(xn), dph = dphi(i, xn) * H;
+  while ((fabs(ph) > kTol) && (fabs(dph) > kTol) && (n < 100)) {
+    p -= ph / dph;
+    xn[i] = PT[i] + p * H;
+    n = n + 1;
+    ph = phi(xn);
+    dph = dphi(i, xn) * H;
+  }
+  if ((n >= 100) || (fabs(dph) <= kTol)) p = bisection(PT, H, i, a, b);
+  return p;
+}
+
+int lu4(double A[4][4], int p[4]) {
+  for (int j = 0; j < 4; j++) p[j] = j;
+  for (int j = 0; j < 4; j++) {
+    int k = j;
+    double m = A[p[j]][j];
+    for (int i = j + 1; i < 4; i++)
+      if (fabs(A[p[i]][j]) > fabs(m)) {
+        m = A[p[i]][j];
+        k = i;
+      }
+    if (k != j) std::swap(p[j], p[k]);
+    double ajj = A[p[j]][j];
+    if (fabs(ajj) < 1.0e-15) return -1;
+    for (int i = j + 1; i < 4; i++) {
+      double lij = A[p[i]][j] / ajj;
+      A[p[i]][j] = lij;
+      for (int kk = j + 1; kk < 4; kk++) A[p[i]][kk] -= lij * A[p[j]][kk];
+    }
+  }
+  return 0;
+}
+void lu4_solve(const double A[4][4], const int p[4], const double b[4], double x[4]) {
+  x[0] = b[p[0]];
+  for (int i = 1; i < 4; i++) {
+    x[i] = b[p[i]];
+    double rs = 0.0;
+    for (int j = 0; j < i; j++) rs += A[p[i]][j] * x[j];
+    x[i] -= rs;
+  }
+  x[3] = x[3] / A[p[3]][3];
+  for (int i = 2; i >= 0; i--) {
+    double rs = 0.0;
+    for (int j = 3; j > i; j--) rs += A[p[i]][j] * x[j];
+    x[i] = (x[i] - rs) / A[p[i]][i];
+  }
+}
+
+// find_Nearest: E2G/surface.cpp:204-295
+int find_nearest(const double* pt, const double* start, double* x0, double* n0) {
+  double x[3] = {start[0], start[1], start[2]};
+  double F[4] = {phi(x), x[0] - pt[0], x[1] - pt[1], x[2] - pt[2]};
+  double Fn = F[0] * F[0] + F[1] * F[1] + F[2] * F[2] + F[3] * F[3];
+  int n = 0;
+  double lam = 0.0;
+  const double H00 = 2.0 / (kAx[0] * kAx[0]), H11 = 2.0 / (kAx[1] * kAx[1]), H22 = 2.0 / (kAx[2] * kAx[2]);
+  while ((Fn > kTol) && (n <= 100)) {
+    double p1 = dphi(0, x), p2 = dphi(1, x), p3 = dphi(2, x);
+    F[0] = phi(x);
+    F[1] = x[0] - pt[0] + lam * p1;
+    F[2] = x[1] - pt[1] + lam * p2;
+    F[3] = x[2] - pt[2] + lam * p3;
+    Fn = F[0] * F[0] + F[1] * F[1] + F[2] * F[2] + F[3] * F[3];
+    double J[4][4] = {{0.0, p1, p2, p3},
+                      {p1, 1.0 + lam * H00, lam * 0.0, lam * 0.0},
+                      {p2, lam * 0.0, 1.0 + lam * H11, lam * 0.0},
+                      {p3, lam * 0.0, lam * 0.0, 1.0 + lam * H22}};
+    int perm[4];
+    if (lu4(J, perm) == -1) return -1;
+    double sol[4];
+    lu4_solve(J, perm, F, sol);
+    lam = lam - sol[0];
+    for (int i = 0; i < 3; i++) x[i] = x[i] - sol[i + 1];
+    n = n + 1;
+  }
+  if (n > 100) return -1;
+  for (int k = 0; k < 3; k++) x0[k] = x[k];
+  double a = dphi(0, x), b = dphi(1, x), c = dphi(2, x);
+  double nn = sqrt(a * a + b * b + c * c);
+  n0[0] = a / nn;
+  n0[1] = b / nn;
+  n0[2] = c / nn;
+  return 0;
+}
+}  // namespace
+
+// Generate_Surface (E2G/surface.cpp:12-66) + stokeslet_density + find_nrst_surfc.
+void build(Scene& S, int N, double band1, double band2) {
+  S.N = N;
+  S.L = 3.0;
+  S.h = S.L / N;
+  const double h = S.h;
+  const double kappa0 = 4.0, q = 5.0 / 7.0;  // E2G/main.cpp:76-80
+  double kappa = kappa0 * pow(1.0 / 64.0, 1.0 - q);
+  S.delta = kappa * pow(h, q);
+  // quadrature points
+  std::vector<std::vector<double>> per(3 * (2 * N + 1));
+  const double cth = cos(kTheta);
+#pragma omp parallel for schedule(dynamic, 1) collapse(2)
+  for (int i = 0; i < 3; i++)
+    for (int l1 = -N; l1 <= N; l1++) {
+      std::vector<double>& out = per[i * (2 * N + 1) + (l1 + N)];
+      int i1 = i == 0 ? 1 : 0, i2 = i == 2 ? 1 : 2;
+      double A[3] = {0, 0, 0}, B[3] = {0, 0, 0};
+      for (int l2 = -N; l2 <= N; l2++) {
+        A[i1] = l1 * h + kCtr;
+        A[i2] = l2 * h + kCtr;
+        B[i1] = l1 * h + kCtr;
+        B[i2] = l2 * h + kCtr;
+        for (int j = -N; j <= N; j++) {
+          A[i] = j * h + kCtr;
+          B[i] = A[i] + h;
+          int sa = phi(A) < 0.0 ? -1 : 1, sb = phi(B) < 0.0 ? -1 : 1;
+          if (sa * sb < 0) {
+            double tau = newton(A, h, i, 0, 1);
+            double x[3] = {A[0], A[1], A[2]};
+            x[i] += tau * h;
+            double nv[3];
+            for (int k = 0; k < 3; k++) nv[k] = dphi(k, x);
+            double nn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+            for (int k = 0; k < 3; k++) nv[k] /= nn;
+            if (fabs(nv[i]) >= cth) {
+              double ar = h * h * part_unity(i, nv) / fabs(nv[i]);
+              out.insert(out.end(), {x[0], x[1], x[2], nv[0], nv[1], nv[2], ar});
+            }
+          }
+        }
+      }
+    }
+  for (auto& v : per)
+    for (size_t k = 0; k < v.size(); k += 7) {
+      S.xq.insert(S.xq.end(), {v[k], v[k + 1], v[k + 2]});
+      S.nrm.insert(S.nrm.end(), {v[k + 3], v[k + 4], v[k + 5]});
+      S.area.push_back(v[k + 6]);
+    }
+  const int nq = (int)S.area.size();
+  S.f.resize(3 * (size_t)nq);
+  for (int j = 0; j < nq; j++) stokeslet_density(&S.xq[3 * j], &S.f[3 * j]);
+  // band tagging: first quadrature point (in order) within (BAND1+1)h of a grid point
+  const long M = N + 1;
+  std::vector<std::atomic<int>> claim(M * M * M);
+  for (auto& c : claim) c.store(nq, std::memory_order_relaxed);
+  const double tol = 1.e-12;
+  const int width = (int)ceil(band1);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int q2 = 0; q2 < nq; q2++) {
+    const double* xs = &S.xq[3 * q2];
+    int i0 = (int)floor(xs[0] / h - band1) - 1;
+    int j0 = (int)floor(xs[1] / h - band1) - 1;
+    int k0 = (int)floor(xs[2] / h - band1) - 1;
+    for (int i = i0; i <= i0 + 2 * width + 3; i++)
+      for (int j = j0; j <= j0 + 2 * width + 3; j++)
+        for (int k = k0; k <= k0 + 2 * width + 3; k++) {
+          if (i < 0 || j < 0 || k < 0 || i > N || j > N || k > N) continue;
+          double pt[3] = {i * h, j * h, k * h};
+          double d_sq = (pt[0] - xs[0]) * (pt[0] - xs[0]) + (pt[1] - xs[1]) * (pt[1] - xs[1]) +
+                        (pt[2] - xs[2]) * (pt[2] - xs[2]);
+          if (sqrt(d_sq) <= ((band1 + 1) * h + tol)) {
+            std::atomic<int>& c = claim[((long)i * M + j) * M + k];
+            int cur = c.load(std::memory_order_relaxed);
+            while (q2 < cur && !c.compare_exchange_weak(cur, q2, std::memory_order_relaxed)) {
+            }
+          }
+        }
+  }
+  struct Tag {
+    int q;
+    long g;
+    double b, x0[3], n0[3];
+  };
+  std::vector<long> cand;
+  for (long g = 0; g < M * M * M; g++)
+    if (claim[g].load(std::memory_order_relaxed) < nq) cand.push_back(g);
+  std::vector<Tag> tags(cand.size());
+  std::vector<uint8_t> ok(cand.size(), 0);
+#pragma omp parallel for schedule(dynamic, 256)
+  for (long c = 0; c < (long)cand.size(); c++) {
+    long g = cand[c];
+    int i = (int)(g / (M * M)), j = (int)((g / M) % M), k = (int)(g % M);
+    double pt[3] = {i * h, j * h, k * h};
+    Tag t;
+    t.q = claim[g].load(std::memory_order_relaxed);
+    t.g = g;
+    if (find_nearest(pt, &S.xq[3 * t.q], t.x0, t.n0) != 0) continue;
+    t.b = (pt[0] - t.x0[0]) * t.n0[0] + (pt[1] - t.x0[1]) * t.n0[1] + (pt[2] - t.x0[2]) * t.n0[2];
+    if (fabs(t.b) <= (band1 * h + tol)) {
+      tags[c] = t;
+      ok[c] = 1;
+    }
+  }
+  std::vector<Tag> kept;
+  for (size_t c = 0; c < cand.size(); c++)
+    if (ok[c]) kept.push_back(tags[c]);
+  // reference order: by claiming quadrature point, then the i, j, k loop
+  std::stable_sort(kept.begin(), kept.end(), [](const Tag& a, const Tag& b) {
+    return a.q != b.q ? a.q < b.q : a.g < b.g;
+  });
+  S.nrst.assign(M * M * M, -1);
+  for (size_t t = 0; t < kept.size(); t++) {
+    S.nrst[kept[t].g] = (int)t;
+    S.b.push_back(kept[t].b);
+    S.x0.insert(S.x0.end(), {kept[t].x0[0], kept[t].x0[1], kept[t].x0[2]});
+    S.n0.insert(S.n0.end(), {kept[t].n0[0], kept[t].n0[1], kept[t].n0[2]});
+    S.band2.push_back(fabs(kept[t].b) <= band2 * h + tol ? 1 : 0);
+  }
+}
+
+}  // namespace e2g_setup

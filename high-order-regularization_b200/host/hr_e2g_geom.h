@@ -1,0 +1,22 @@
+// hr_e2g_geom.h — host setup of the extend-to-grid problem (internal).
+#pragma once
+#include <cstdint>
+#include <vector>
+
+namespace e2g_setup {
+
+struct Scene {
+  int N = 0;
+  double L = 3.0, h = 0, delta = 0;
+  std::vector<double> xq, nrm, area, f;  // quadrature points, normals, areas, exact density
+  std::vector<int> nrst;                 // (N+1)^3: tagged target index or -1
+  std::vector<double> b, x0, n0;         // per tagged target
+  std::vector<uint8_t> band2;
+};
+
+void build(Scene& S, int N, double band1, double band2);
+void stokeslet_density(const double* pt, double* f);
+double p_exact(double x, double y, double z);
+void u_exact(double x, double y, double z, double* u);
+
+}  // namespace e2g_setup

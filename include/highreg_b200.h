@@ -132,6 +132,43 @@ int hr_dst_poisson3d(hr_ctx* ctx, int n, double* f);
 int hr_e2g_solve_poisson(hr_ctx* ctx, int N, double L, const uint8_t* band2,
                          const uint8_t* outside, const double* p, double* u, int variable);
 
+/* ---------------------------------------------- extend-to-grid pipeline */
+/* The whole extend-to-grid computation of test_Stokes_Poisson3d_FD
+ * (E2G/main.cpp:107-424) for the translating prolate spheroid on [0, 3]^3,
+ * h = 3/N: host setup (Generate_Surface, find_nrst_surfc with BAND1 = 4,
+ * BAND2 = 2, exact density) at create time; on the device, the face and band
+ * pressure / velocity sums in one batched launch, then the four Poisson
+ * extensions (p, then u with the extended p). N must be even and >= 36. */
+typedef struct hr_e2g hr_e2g;
+typedef struct {
+  int N;
+  double L, h, delta;
+  int nq;        /* quadrature points */
+  int n_tagged;  /* grid points within BAND1 of the surface */
+  int n_band;    /* tagged interior points outside or on the surface (evaluated) */
+  int n_face;    /* box-face grid points */
+  long long pairs;
+} hr_e2g_info;
+typedef struct {
+  double seconds_sums;     /* the four boundary sums */
+  double seconds_poisson;  /* the four Poisson extensions */
+  double seconds_total;
+  long long pairs;
+} hr_e2g_report;
+int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out);
+int hr_e2g_get_info(const hr_e2g* e, hr_e2g_info* info);
+int hr_e2g_run(hr_e2g* e, int precision, hr_e2g_report* rep);
+/* which: 0 p after the sums, 1 u after the sums (3 grids), 2 extended p,
+ * 3 extended u (3 grids); grids row-major (N+1)^3 */
+int hr_e2g_get(hr_e2g* e, int which, double* out);
+/* which: 0 quadrature (3nq xyz, 3nq nrml, nq area, 3nq f), 1 nrst grid (int,
+ * (N+1)^3), 2 tagged targets (b, 3 x0, 3 n0, band2) as doubles */
+int hr_e2g_scene(const hr_e2g* e, int which, void* out);
+void hr_e2g_destroy(hr_e2g* e);
+/* exact translating-spheroid solution (E2G/utilities.cpp:294-411) */
+double hr_e2g_p_exact(double x, double y, double z);
+void hr_e2g_u_exact(double x, double y, double z, double* u);
+
 /* --------------------------------------------------- two-surface problem */
 /* The two-surface boundary integral equation (I - 2/3 D) u = b
  * (2S/main.cpp:140-417). Target set s is the quadrature points of surface s
