@@ -255,6 +255,7 @@ def run_ours(args, rank, world, local_rank):
     # dominant kernel: the stresslet batch of the operator (one launch per matvec)
     plan.matvec_dev(x, b)
     ms_dl = plan.time_batch(0, 20)
+    ms_dl_mixed = plan.time_batch(2, 20)
     moment_flops = 2.0 * 12 * w_mv["moment_terms"]
     fl_launch = w_mv["flops"] - moment_flops
     peak = ctx.fp64_peak()
@@ -263,6 +264,7 @@ def run_ours(args, rank, world, local_rank):
                 "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None,
                 "flops_per_launch": fl_launch, "ms_per_launch": ms_dl,
+                "ms_per_launch_mixed_precision": ms_dl_mixed,
                 "peak_source": "measured FP64 FMA loop (hr_measure_fp64_peak) on this GPU"}
 
     # end to end through the C ABI with host buffers: scene upload + plan

@@ -17,6 +17,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhighreg_b200.so")
+REFAPI = os.path.join(HERE, "libhighreg_refapi.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp",
@@ -26,7 +27,7 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-I", os.path.joi
 
 def _sources():
     cu = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
-    cpp = sorted(glob.glob(os.path.join(HERE, "host", "*.cpp")))
+    cpp = sorted(f for f in glob.glob(os.path.join(HERE, "host", "*.cpp")) if not f.endswith("hr_ref_api.cpp"))
     hdr = sorted(glob.glob(os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh"))
                  + glob.glob(os.path.join(HERE, "host", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h")))
     return cu, cpp, hdr
@@ -61,6 +62,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcufft", "-Xcompiler", "-fopenmp", "-lgomp"]
         logs.append(_run(cmd, verbose))
+    # the reference-signature layer, a separate library over the C ABI
+    src = os.path.join(HERE, "host", "hr_ref_api.cpp")
+    if force or not os.path.exists(REFAPI) or os.path.getmtime(REFAPI) < max(os.path.getmtime(src), hdr_t,
+                                                                              os.path.getmtime(LIB)):
+        logs.append(_run(["g++"] + CXXFLAGS + ["-shared", src, "-o", REFAPI, "-L", HERE, "-lhighreg_b200",
+                          "-Wl,-rpath,$ORIGIN"], verbose))
     if ptxas_info:
         print("\n".join(l for l in logs if l))
     return LIB

@@ -320,6 +320,14 @@ void build(Scene& S, int N, double band1, double band2) {
   std::vector<long> cand;
   for (long g = 0; g < M * M * M; g++)
     if (claim[g].load(std::memory_order_relaxed) < nq) cand.push_back(g);
+  // quadrature points bucketed by grid cell, for the retries below
+  std::vector<std::pair<long, int>> cells(nq);
+  auto cell_key = [&](long a, long b2, long c) { return (a * (M + 16) + b2) * (M + 16) + c; };
+  for (int q2 = 0; q2 < nq; q2++) {
+    const double* xs = &S.xq[3 * q2];
+    cells[q2] = {cell_key((long)floor(xs[0] / h) + 8, (long)floor(xs[1] / h) + 8, (long)floor(xs[2] / h) + 8), q2};
+  }
+  std::sort(cells.begin(), cells.end());
   std::vector<Tag> tags(cand.size());
   std::vector<uint8_t> ok(cand.size(), 0);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -328,11 +336,43 @@ void build(Scene& S, int N, double band1, double band2) {
     int i = (int)(g / (M * M)), j = (int)((g / M) % M), k = (int)(g % M);
     double pt[3] = {i * h, j * h, k * h};
     Tag t;
-    t.q = claim[g].load(std::memory_order_relaxed);
     t.g = g;
-    if (find_nearest(pt, &S.xq[3 * t.q], t.x0, t.n0) != 0) continue;
-    t.b = (pt[0] - t.x0[0]) * t.n0[0] + (pt[1] - t.x0[1]) * t.n0[1] + (pt[2] - t.x0[2]) * t.n0[2];
-    if (fabs(t.b) <= (band1 * h + tol)) {
+    t.q = claim[g].load(std::memory_order_relaxed);
+    auto attempt = [&](int q2) {
+      if (find_nearest(pt, &S.xq[3 * q2], t.x0, t.n0) != 0) return false;
+      t.b = (pt[0] - t.x0[0]) * t.n0[0] + (pt[1] - t.x0[1]) * t.n0[1] + (pt[2] - t.x0[2]) * t.n0[2];
+      return fabs(t.b) <= (band1 * h + tol);
+    };
+    bool tagged = attempt(t.q);
+    if (!tagged) {
+      // The reference leaves the point untagged and tries again from every
+      // later quadrature point whose neighbourhood contains it
+      // (E2G/surface.cpp:325-358): same candidates, same order.
+      std::vector<int> later;
+      for (long a = i - 7; a <= i + 7; a++)
+        for (long b2 = j - 7; b2 <= j + 7; b2++)
+          for (long c2 = k - 7; c2 <= k + 7; c2++) {
+            long key = cell_key(a + 8, b2 + 8, c2 + 8);
+            auto it = std::lower_bound(cells.begin(), cells.end(), std::make_pair(key, -1));
+            for (; it != cells.end() && it->first == key; ++it) {
+              int q2 = it->second;
+              if (q2 <= t.q) continue;
+              const double* xs = &S.xq[3 * q2];
+              double d_sq = (pt[0] - xs[0]) * (pt[0] - xs[0]) + (pt[1] - xs[1]) * (pt[1] - xs[1]) +
+                            (pt[2] - xs[2]) * (pt[2] - xs[2]);
+              if (sqrt(d_sq) <= ((band1 + 1) * h + tol)) later.push_back(q2);
+            }
+          }
+      std::sort(later.begin(), later.end());
+      for (int q2 : later) {
+        if (attempt(q2)) {
+          t.q = q2;
+          tagged = true;
+          break;
+        }
+      }
+    }
+    if (tagged) {
       tags[c] = t;
       ok[c] = 1;
     }

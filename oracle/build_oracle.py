@@ -116,6 +116,27 @@ def build_reference(force: bool = False) -> list:
     return built
 
 
+def build_relinked_reference(force: bool = False):
+    """The reference's unmodified two-surface driver (main.cpp, surface.cpp,
+    utilities.cpp) linked against the product's reference-signature layer
+    (libhighreg_refapi.so) instead of its own KITC.cpp / stokeslets.cpp /
+    stresslets.cpp: the drop-in test of the C++ boundary. Needs the reference
+    tree and the built product library; returns the binary path or None."""
+    s2 = os.path.join(REF_ROOT, "highreg_stokes_2surf")
+    pkg = os.path.join(os.path.dirname(HERE), "high-order-regularization_b200")
+    lib = os.path.join(pkg, "libhighreg_refapi.so")
+    if not os.path.isdir(s2) or not os.path.exists(lib):
+        return None
+    os.makedirs(REF_OUT, exist_ok=True)
+    out = os.path.join(REF_OUT, "ref2s_main_relinked")
+    srcs = [os.path.join(s2, f) for f in ("main.cpp", "surface.cpp", "utilities.cpp")]
+    if force or not _newer(out, srcs + [lib]):
+        _run(["g++", "-std=c++14", "-O2", "-fopenmp", "-w", "-I", s2] + srcs
+             + ["-o", out, "-L", pkg, "-lhighreg_refapi", "-lhighreg_b200", "-Wl,-rpath," + pkg,
+                "-Wl,-rpath,$ORIGIN/../../high-order-regularization_b200"])
+    return out
+
+
 def build_all(force: bool = False) -> None:
     build_checker(force)
     build_reference(force)

@@ -52,6 +52,18 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_refapi_library_exports_reference_signatures():
+    import subprocess
+
+    lib = os.path.join(ROOT, "high-order-regularization_b200", "libhighreg_refapi.so")
+    out = subprocess.run(["nm", "-DC", lib], capture_output=True, text=True).stdout
+    txt = open(os.path.join(ROOT, "include", "highreg_refapi.h")).read()
+    names = sorted(set(re.findall(r"\b(eval_Stokes_[A-Za-z_]+|hr_refapi_[a-z_]+)\s*\(", txt)))
+    assert len(names) == 11
+    for n in names:
+        assert re.search(r" T " + n + r"\b", out), n
+
+
 def test_context_argument_errors():
     L = highreg.lib()
     assert L.hr_ctx_create(0, None) == highreg.HR_ERR_ARG
