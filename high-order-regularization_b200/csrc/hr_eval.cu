@@ -257,7 +257,16 @@ __device__ __forceinline__ void pair32(const float* __restrict__ sf, int j, cons
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = rsqrtf(r2);
   const float rinv2 = rinv * rinv;
-  if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7 || KIND == K_E2G_SL_AWAY) {
+  if (KIND == K_E2G_SL_AWAY) {
+    // plain Stokeslet, no subtraction; the face sums stage no normals
+    const float fx = QX[j], fy = QY[j], fz = QZ[j];
+    const float fdd = fx * dx + fy * dy + fz * dz;
+    const float H1 = A[j] * rinv;
+    const float H2 = fdd * H1 * rinv2;
+    p0 += fx * H1 + dx * H2;
+    p1 += fy * H1 + dy * H2;
+    p2 += fz * H1 + dz * H2;
+  } else if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7) {
     const float fx = QX[j] - F.f0n0 * NX[j];
     const float fy = QY[j] - F.f0n0 * NY[j];
     const float fz = QZ[j] - F.f0n0 * NZ[j];
