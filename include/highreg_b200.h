@@ -265,6 +265,24 @@ void hr_geom2s_destroy(hr_geom2s* g);
 /* Runs an FP64 FMA throughput loop on the device; returns FLOP/s. */
 int hr_measure_fp64_peak(hr_ctx* ctx, double* flops_per_s);
 
+/* -------------------------------------- allocation-free Stokeslet sum */
+/* No counterpart in the reference. The plain Stokeslet sum of
+ * hr_e2g_stokeslet_away (all pairs, scaled by 1/(8 pi)) on caller-owned
+ * DEVICE buffers, with no device allocation and no context: for callers that
+ * cannot call cudaMalloc (a memory pool or framework allocator owns the
+ * device, or the path must not synchronize the device as cudaMalloc/cudaFree
+ * may). Its only scratch, 3 doubles per (target, source chunk), is a
+ * file-scope __device__ array of 4 Mi doubles (32 MiB per device), so nt is
+ * limited to hr_stokeslet_away_noalloc_max_targets() = 1,398,101; larger nt
+ * returns HR_ERR_ARG. The first call on a device (that device current) looks
+ * the array up once; make it before any stream capture. All calls share the
+ * array and leave their partial sums in it; every slot read is written
+ * first, so nothing needs clearing, but calls that overlap on the GPU race.
+ * Enqueued on `stream` (a cudaStream_t, NULL = legacy default stream). */
+int hr_stokeslet_away_noalloc(const double* xyz_src_dev, const double* area_dev, const double* f_dev, int nq,
+                              const double* xyz_tgt_dev, int nt, double* out_dev, void* stream);
+long long hr_stokeslet_away_noalloc_max_targets(void);
+
 #ifdef __cplusplus
 }
 #endif
