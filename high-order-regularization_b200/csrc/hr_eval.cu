@@ -12,13 +12,13 @@
 //                    in shared memory (Call_Treecode_*, 2S/KITC.cpp:671-777).
 // A warp whose mask word is zero for an entry skips the arithmetic entirely.
 //
-// Precision. FP64: every pair in FP64. MIXED: pairs that are well separated
-// in the reference's own sense (every pair of a target with |b|/delta > 8, the
-// r > 8 delta pairs of targets that use the regularized kernels, and all
-// proxy interactions) are evaluated in FP32 from centre-relative FP32
-// coordinates, summed per tile in FP32 and added to the FP64 per-target
-// accumulators; the r <= 8 delta pairs (erf/exp smoothing, subtraction) and
-// every pair of a near off-surface stresslet target stay in FP64.
+// Precision. FP64: every pair in FP64. MIXED: every pair with r > 3 delta is
+// evaluated in FP32 from centre-relative FP32 coordinates (the plain kernels
+// of far targets, the regularized kernels with erff/expf for 3 delta < r <=
+// 8 delta, the subtraction forms of near targets, and all proxy
+// interactions), summed per 16 terms in FP32 and added to the FP64
+// per-target accumulators; the r <= 3 delta pairs, where the smoothing
+// brackets cancel, stay in FP64.
 #include <cstdio>
 
 #include "hr_device.h"
@@ -47,6 +47,10 @@ struct Tgt32 {
   float f0n0;        // 0 for targets without subtraction
   float g0[3];
   float n0xf0[3];
+  float b;
+  float x0[3];       // relative to the source surface centre
+  float n0[3];
+  CoefF c;
 };
 
 template <int KIND>
@@ -103,12 +107,20 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
   F.px = (float)(S.px - T.ctr[0]);
   F.py = (float)(S.py - T.ctr[1]);
   F.pz = (float)(S.pz - T.ctr[2]);
-  // the direct sum of a far Stokeslet target has no subtraction (2S/KITC.cpp:856-882)
+  // the direct sum of a far Stokeslet target has no subtraction (2S/KITC.cpp:856-882),
+  // nor has the plain stresslet of a far target (2S/KITC.cpp:970-995)
   F.f0n0 = (KIND == K_SL_OFF && !S.near) ? 0.0f : (float)S.f0n0;
+  const bool no_g0 = KIND == K_DL_OFF && !S.near;
   for (int k = 0; k < 3; k++) {
-    F.g0[k] = (float)S.g0[k];
+    F.g0[k] = no_g0 ? 0.0f : (float)S.g0[k];
     F.n0xf0[k] = (float)S.n0xf0[k];
+    F.x0[k] = (float)(S.x0[k] - T.ctr[k]);
+    F.n0[k] = (float)S.n0[k];
   }
+  F.b = (float)S.b;
+  F.c.c1 = (float)S.c.c1;
+  F.c.c2 = (float)S.c.c2;
+  F.c.c3 = (float)S.c.c3;
 }
 
 // ---------------------------------------------------------------- FP64 pairs
@@ -305,6 +317,100 @@ __device__ __forceinline__ void pair32(const float* __restrict__ sf, int j, cons
   }
 }
 
+// ------------------------------------------------ FP32 pairs, r > 3 delta
+// The full kernel of a target that uses the regularized forms (the smoothed
+// branch for r <= 8 delta, the singular one beyond, with the target's
+// subtraction), in FP32 for pairs with r > 3 delta. Returns true if the
+// smoothed branch was taken.
+template <int KIND>
+__device__ __forceinline__ bool pair32r(const float* __restrict__ sf, int j, const Tgt32& F, const RegF& gf,
+                                        float& p0, float& p1, float& p2) {
+  const float* X = sf;
+  const float* Y = sf + kNT;
+  const float* Z = sf + 2 * kNT;
+  const float* NX = sf + 3 * kNT;
+  const float* NY = sf + 4 * kNT;
+  const float* NZ = sf + 5 * kNT;
+  const float* A = sf + 6 * kNT;
+  const float* QX = sf + 7 * kNT;
+  const float* QY = sf + 8 * kNT;
+  const float* QZ = sf + 9 * kNT;
+  const float dx = F.px - X[j], dy = F.py - Y[j], dz = F.pz - Z[j];
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = rsqrtf(r2);
+  const bool reg = r2 <= gf.d64;
+  if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7) {
+    const float fx = QX[j] - F.f0n0 * NX[j];
+    const float fy = QY[j] - F.f0n0 * NY[j];
+    const float fz = QZ[j] - F.f0n0 * NZ[j];
+    const float fdd = fx * dx + fy * dy + fz * dz;
+    float H1, H2;
+    if (KIND == K_SL_ON) sl_7ord_onsurf_f(r2, rinv, gf, H1, H2);
+    else sl_7ord_f(r2, rinv, gf, F.c, H1, H2);
+    H1 *= A[j];
+    H2 *= A[j] * fdd;
+    p0 += fx * H1 + dx * H2;
+    p1 += fy * H1 + dy * H2;
+    p2 += fz * H1 + dz * H2;
+  } else if (KIND == K_DL_ON) {
+    const float gx = QX[j] - F.g0[0];
+    const float gy = QY[j] - F.g0[1];
+    const float gz = QZ[j] - F.g0[2];
+    const float gdd = gx * dx + gy * dy + gz * dz;
+    const float ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+    float H3;
+    dl_7ord_onsurf_f(r2, rinv, gf, H3);
+    const float kernel = ndd * gdd * H3 * A[j];
+    p0 += dx * kernel;
+    p1 += dy * kernel;
+    p2 += dz * kernel;
+  } else if (KIND == K_DL_OFF) {
+    // the subtraction form of a near target (2S/KITC.cpp:996-1059)
+    const float b = F.b;
+    const float xh0 = X[j] - F.x0[0], xh1 = Y[j] - F.x0[1], xh2 = Z[j] - F.x0[2];
+    const float gx = QX[j] - F.g0[0], gy = QY[j] - F.g0[1], gz = QZ[j] - F.g0[2];
+    const float sig_sq = (xh0 * xh0 + xh1 * xh1 + xh2 * xh2) - 2.0f * b * (xh0 * F.n0[0] + xh1 * F.n0[1] + xh2 * F.n0[2]);
+    const float g_dot_n0 = gx * F.n0[0] + gy * F.n0[1] + gz * F.n0[2];
+    const float g_dot_xh = gx * xh0 + gy * xh1 + gz * xh2;
+    const float n0_dot_n = F.n0[0] * NX[j] + F.n0[1] * NY[j] + F.n0[2] * NZ[j];
+    const float xh_dot_n = xh0 * NX[j] + xh1 * NY[j] + xh2 * NZ[j];
+    const float c_m1a = g_dot_n0 * n0_dot_n;
+    const float c_m1b = g_dot_xh * n0_dot_n + g_dot_n0 * xh_dot_n;
+    const float c_m2a = g_dot_xh * xh_dot_n;
+    const float c_m2b = b * c_m1b;
+    float H2, H3;
+    dl_7ord_f(r2, rinv, gf, F.c, H2, H3);
+    H2 *= A[j];
+    H3 *= A[j];
+    float m1 = dx * c_m1a - F.n0[0] * c_m1b;
+    float m2 = -sig_sq * m1 + dx * c_m2a + xh0 * c_m2b;
+    p0 += m1 * H2 + m2 * H3;
+    m1 = dy * c_m1a - F.n0[1] * c_m1b;
+    m2 = -sig_sq * m1 + dy * c_m2a + xh1 * c_m2b;
+    p1 += m1 * H2 + m2 * H3;
+    m1 = dz * c_m1a - F.n0[2] * c_m1b;
+    m2 = -sig_sq * m1 + dz * c_m2a + xh2 * c_m2b;
+    p2 += m1 * H2 + m2 * H3;
+  } else if (KIND == K_E2G_P7) {
+    float H2;
+    lapl_dl_7ord_f(r2, rinv, gf, F.c, H2);
+    const float n0 = NX[j], n1 = NY[j], n2 = NZ[j];
+    const float f0 = QX[j], f1 = QY[j], f2 = QZ[j];
+    const float f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
+    const float ncf0 = (n1 * f2 - n2 * f1) - F.n0xf0[0];
+    const float ncf1 = (n2 * f0 - n0 * f2) - F.n0xf0[1];
+    const float ncf2 = (n0 * f1 - n1 * f0) - F.n0xf0[2];
+    const float n_dot_dx = n0 * dx + n1 * dy + n2 * dz;
+    const float ncd0 = n1 * dz - n2 * dy;
+    const float ncd1 = n2 * dx - n0 * dz;
+    const float ncd2 = n0 * dy - n1 * dx;
+    const float normal = -(f_dot_n - F.f0n0) * n_dot_dx;
+    const float tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
+    p0 += (normal + tangential) * H2 * A[j];
+  }
+  return reg;
+}
+
 // ------------------------------------------------------------ proxy tiles
 
 template <bool DL>
@@ -414,13 +520,16 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   Tgt32 F;
   load_target<KIND>(T, t, valid, S, F);
   const Reg g = make_reg(T.DEL);
-  const float d64f = (float)g.d64;
+  RegF gf;
+  gf.inv_d = (float)g.inv_d;
+  gf.d64 = (float)g.d64;
+  const float cut2f = (float)(9.0 * T.DEL * T.DEL);  // (3 delta)^2: FP64 below, FP32 above
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   unsigned long long creg = 0, cplain = 0, cfar = 0, cprox = 0;
   constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY);
   // which path a target takes through a source tile
-  constexpr bool kPerPairSplit =
-      (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7 || KIND == K_E2G_P7);
+  constexpr bool kPerPairSplit = (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_SL_OFF || KIND == K_DL_OFF ||
+                                   KIND == K_E2G_SL7 || KIND == K_E2G_P7);
   const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY ||
                                ((KIND == K_SL_OFF || KIND == K_DL_OFF) && !S.near));
   for (int q = it.seg0; q < it.seg1; q++) {
@@ -482,7 +591,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
               const int j1 = min(cnt, j0 + 16);
               for (int j = j0; j < j1; j++) {
                 const float dx = F.px - sf[j], dy = F.py - sf[kNT + j], dz = F.pz - sf[2 * kNT + j];
-                if (dx * dx + dy * dy + dz * dz > d64f) pair32<KIND>(sf, j, F, p0, p1, p2);
+                if (dx * dx + dy * dy + dz * dz > cut2f) cr += pair32r<KIND>(sf, j, F, gf, p0, p1, p2);
                 else cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
               }
               a0 += (double)p0;

@@ -196,3 +196,104 @@ __device__ __forceinline__ bool lapl_dl_7ord(double r2, double rinv, const Reg& 
 }
 
 }  // namespace hr
+
+// ------------------------------------------------------------------ FP32 forms
+// The same kernels in FP32 for the mixed-precision path, used only for pairs
+// with r > 3 delta. There, for every target distance |b| <= 8 delta (the
+// coefficients c1..c3 of reg_coeff) the brackets erf + poly * (r/delta)
+// exp(-r^2/delta^2) of s1, s2 and s3 satisfy
+// (|erf| + |poly * ...|) / |bracket| < 1.005, so no term cancels and FP32
+// keeps ~1e-7 relative accuracy per pair; at 2.5 delta that factor is 1.8, at
+// 2 delta 11, and as r -> 0 the s2 / s3 brackets cancel to O((r/delta)^3),
+// which is why closer pairs stay in FP64. erff and expf are CUDA's own
+// functions.
+namespace hr {
+
+struct RegF {
+  float inv_d, d64;  // 1/delta, 64 delta^2
+};
+
+struct CoefF {
+  float c1, c2, c3;
+};
+
+constexpr float kRootPiF = 1.77245385f;
+
+__device__ __forceinline__ void sl_7ord_f(float r2, float rinv, const RegF& g, const CoefF& c, float& s1,
+                                          float& s2) {
+  const float rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s1 = rinv;
+    s2 = rinv3;
+    return;
+  }
+  const float rd = r2 * rinv * g.inv_d, rd2 = rd * rd, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const float errfn = erff(rd), r_expfn = rd * expf(-rd2);
+  const float poly1 = c.c1 - 2.0f * (c.c2 + c.c3) * rd2 + 4.0f * c.c3 * rd4;
+  const float poly2 = -2.0f / kRootPiF + 2.0f * (c.c1 + 2.0f * (c.c2 + c.c3)) * rd2 -
+                      4.0f * (c.c2 + 5.0f * c.c3) * rd4 + 8.0f * c.c3 * rd6;
+  s1 = (errfn + poly1 * r_expfn) * rinv;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+}
+
+__device__ __forceinline__ void sl_7ord_onsurf_f(float r2, float rinv, const RegF& g, float& s1, float& s2) {
+  const float rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s1 = rinv;
+    s2 = rinv3;
+    return;
+  }
+  const float rd = r2 * rinv * g.inv_d, rd2 = rd * rd, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const float errfn = erff(rd), r_expfn = 2.0f / kRootPiF * rd * expf(-rd2);
+  const float poly1 = 11.0f / 5.0f - 26.0f / 15.0f * rd2 + 4.0f / 15.0f * rd4;
+  const float poly2 = -1.0f + (118.0f * rd2 - 68.0f * rd4 + 8.0f * rd6) * (1.0f / 15.0f);
+  s1 = (errfn + poly1 * r_expfn) * rinv;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+}
+
+__device__ __forceinline__ void dl_7ord_f(float r2, float rinv, const RegF& g, const CoefF& c, float& s2,
+                                          float& s3) {
+  const float rinv2 = rinv * rinv, rinv3 = rinv2 * rinv;
+  if (r2 > g.d64) {
+    s2 = rinv3;
+    s3 = rinv3 * rinv2;
+    return;
+  }
+  const float rd = r2 * rinv * g.inv_d, rd2 = rd * rd, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const float errfn = erff(rd), r_expfn = rd * expf(-rd2);
+  const float poly2 = -2.0f / kRootPiF + 2.0f * (c.c1 + 2.0f * (c.c2 + c.c3)) * rd2 -
+                      4.0f * (c.c2 + 5.0f * c.c3) * rd4 + 8.0f * c.c3 * rd6;
+  const float poly3 = -2.0f / kRootPiF * (1.0f + 2.0f / 3.0f * rd2) +
+                      4.0f / 3.0f *
+                          ((c.c1 + 4.0f * c.c2 + 12.0f * c.c3) * rd4 - 2.0f * (c.c2 + 9.0f * c.c3) * rd6 +
+                           4.0f * c.c3 * rd6 * rd2);
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  s3 = (errfn + poly3 * r_expfn) * (rinv3 * rinv2);
+}
+
+__device__ __forceinline__ void dl_7ord_onsurf_f(float r2, float rinv, const RegF& g, float& s3) {
+  const float rinv2 = rinv * rinv, rinv5 = rinv2 * rinv2 * rinv;
+  if (r2 > g.d64) {
+    s3 = rinv5;
+    return;
+  }
+  const float rd = r2 * rinv * g.inv_d, rd2 = rd * rd, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const float errfn = erff(rd), r_expfn = 2.0f / kRootPiF * rd * expf(-rd2);
+  const float poly3 = -1.0f - 2.0f / 3.0f * rd2 + 52.0f / 45.0f * rd4 - 8.0f / 45.0f * rd6;
+  s3 = (errfn + poly3 * r_expfn) * rinv5;
+}
+
+__device__ __forceinline__ void lapl_dl_7ord_f(float r2, float rinv, const RegF& g, const CoefF& c, float& s2) {
+  const float rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s2 = rinv3;
+    return;
+  }
+  const float rd = r2 * rinv * g.inv_d, rd2 = rd * rd, rd4 = rd2 * rd2;
+  const float errfn = erff(rd), r_expfn = rd * expf(-rd2);
+  const float poly2 = -2.0f / kRootPiF + 2.0f * (c.c1 + 2.0f * (c.c2 + c.c3)) * rd2 -
+                      4.0f * (c.c2 + 5.0f * c.c3) * rd4 + 8.0f * c.c3 * rd4 * rd2;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+}
+
+}  // namespace hr

@@ -55,7 +55,8 @@ class Scene2S(ctypes.Structure):
 
 class GmresOpts(ctypes.Structure):
     _fields_ = [("restart", ctypes.c_int), ("max_iter", ctypes.c_int), ("tol", ctypes.c_double),
-                ("precision", ctypes.c_int), ("use_guess", ctypes.c_int), ("true_residual", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("use_guess", ctypes.c_int), ("true_residual", ctypes.c_int),
+                ("mixed_accuracy", ctypes.c_double)]
 
 
 class GmresReport(ctypes.Structure):
@@ -84,7 +85,7 @@ class Work(ctypes.Structure):
 class Geom2SParams(ctypes.Structure):
     _fields_ = [("axes", ctypes.c_double * 3), ("center", (ctypes.c_double * 3) * 2),
                 ("unrot", (ctypes.c_double * 9) * 2), ("rotated", ctypes.c_int * 2),
-                ("kappa0", ctypes.c_double), ("q", ctypes.c_double)]
+                ("kappa0", ctypes.c_double), ("q", ctypes.c_double), ("tension_body", ctypes.c_int)]
 
 
 _lib = None
@@ -374,10 +375,12 @@ def scene_struct(keep, geo):
     return sc
 
 
-def gmres_opts(restart=15, max_iter=100, tol=1e-10, precision=HR_FP64, use_guess=False, true_residual=False):
+def gmres_opts(restart=15, max_iter=100, tol=1e-10, precision=HR_FP64, use_guess=False, true_residual=False,
+               mixed_accuracy=0.0):
     o = GmresOpts()
     o.restart, o.max_iter, o.tol, o.precision = restart, max_iter, tol, precision
     o.use_guess, o.true_residual = int(bool(use_guess)), int(bool(true_residual))
+    o.mixed_accuracy = mixed_accuracy
     return o
 
 
@@ -521,3 +524,124 @@ def e2g_exact(x, y, z):
     u = np.zeros(3)
     L.hr_e2g_u_exact(ctypes.c_double(x), ctypes.c_double(y), ctypes.c_double(z), _dp(u))
     return L.hr_e2g_p_exact(ctypes.c_double(x), ctypes.c_double(y), ctypes.c_double(z)), u
+
+
+# ---------------------------------------------------------------- warm start
+NFEAT = 12
+
+
+class WarmInstance(ctypes.Structure):
+    _fields_ = [("geom", Geom2SParams), ("U", ctypes.c_double * 3), ("Omega", ctypes.c_double * 3),
+                ("xmid", ctypes.c_double * 3), ("gap", ctypes.c_double)]
+
+    def as_dict(self):
+        return dict(U=list(self.U), Omega=list(self.Omega), xmid=list(self.xmid), gap=self.gap,
+                    center2=list(self.geom.center[1]), unrot2=list(self.geom.unrot[1]))
+
+
+def warm_instance(seed: int, index: int) -> WarmInstance:
+    """Seeded two-surface instance (random gap, orientation, rigid motion)."""
+    w = WarmInstance()
+    rc = lib().hr_warm_instance_make(ctypes.c_ulonglong(seed), index, ctypes.byref(w))
+    if rc != HR_OK:
+        raise HrError(rc, "hr_warm_instance_make failed")
+    return w
+
+
+def warm_features(geo: dict, inst: WarmInstance):
+    """(features float32 [n, 12], imposed velocity float64 [3n]) of a scene."""
+    keep = _Keep()
+    sc = scene_struct(keep, geo)
+    n = len(geo["area0"]) + len(geo["area1"])
+    feat = np.zeros((n, NFEAT), np.float32)
+    u = np.zeros(3 * n)
+    rc = lib().hr_warm_features(ctypes.byref(sc), ctypes.byref(inst),
+                                feat.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), _dp(u))
+    if rc != HR_OK:
+        raise HrError(rc, "hr_warm_features failed")
+    return feat, u
+
+
+def warm_frames(inst: WarmInstance):
+    """Body frames of the two surfaces: (2, 3, 3), v_body = R v_world."""
+    rot = np.zeros(18)
+    rc = lib().hr_warm_frames(ctypes.byref(inst), _dp(rot))
+    if rc != HR_OK:
+        raise HrError(rc, "hr_warm_frames failed")
+    return rot.reshape(2, 3, 3)
+
+
+def _fdev(t):
+    return ctypes.cast(ctypes.c_void_p(t.data_ptr()), ctypes.POINTER(ctypes.c_float))
+
+
+class MLP:
+    """The warm-start network on the device (hand-written CUDA kernels)."""
+
+    NPARAMS = 9347
+
+    def __init__(self, ctx: Context, seed: int = 0):
+        self.ctx = ctx
+        L = lib()
+        L.hr_mlp_destroy.restype = None
+        p = ctypes.c_void_p()
+        ctx._check(L.hr_mlp_create(ctx.p, ctypes.c_ulonglong(seed), ctypes.byref(p)))
+        self.p = p
+
+    def __del__(self):
+        if getattr(self, "p", None):
+            lib().hr_mlp_destroy(self.p)
+            self.p = None
+
+    def set_normalization(self, mean, std, out_scale):
+        m = np.ascontiguousarray(mean, np.float32)
+        s = np.ascontiguousarray(std, np.float32)
+        fp = ctypes.POINTER(ctypes.c_float)
+        self.ctx._check(lib().hr_mlp_set_normalization(self.p, m.ctypes.data_as(fp), s.ctypes.data_as(fp),
+                                                       ctypes.c_float(out_scale)))
+
+    def params(self):
+        out = np.zeros(self.NPARAMS, np.float32)
+        self.ctx._check(lib().hr_mlp_get_params(self.p, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def set_params(self, p):
+        a = np.ascontiguousarray(p, np.float32)
+        self.ctx._check(lib().hr_mlp_set_params(self.p, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def train_step(self, X, T, batch, lr, seed=0, random=True, want_loss=False):
+        """X, T: torch CUDA float32 tensors (n x 12, n x 3)."""
+        loss = ctypes.c_double()
+        self.ctx._check(lib().hr_mlp_train_step(self.p, _fdev(X), _fdev(T), ctypes.c_long(X.shape[0]), batch,
+                                                1 if random else 0, ctypes.c_ulonglong(seed), ctypes.c_float(lr),
+                                                ctypes.byref(loss) if want_loss else None))
+        return loss.value if want_loss else None
+
+    def gradient(self, X, T, batch):
+        g = np.zeros(self.NPARAMS, np.float32)
+        loss = ctypes.c_double()
+        self.ctx._check(lib().hr_mlp_gradient(self.p, _fdev(X), _fdev(T), batch,
+                                              g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(loss)))
+        return loss.value, g
+
+    def infer(self, X, out=None, base=None, raw=None):
+        """X: torch CUDA float32 (n x 12); out/base: float64 (3n); raw: float32 (n x 3)."""
+        self.ctx._check(lib().hr_mlp_infer(self.p, _fdev(X), ctypes.c_long(X.shape[0]),
+                                           None if base is None else _devp(base),
+                                           None if out is None else _devp(out),
+                                           None if raw is None else _fdev(raw)))
+
+    def infer_frames(self, X, out, base, starts, rot):
+        """Body-frame output rotated back: starts (nframes + 1 offsets), rot (nframes, 3, 3)."""
+        st = np.ascontiguousarray(starts, np.int64)
+        r = np.ascontiguousarray(rot, np.float64).reshape(-1)
+        self.ctx._check(lib().hr_mlp_infer_frames(self.p, _fdev(X), ctypes.c_long(X.shape[0]),
+                                                  None if base is None else _devp(base), _devp(out),
+                                                  len(st) - 1, st.ctypes.data_as(ctypes.POINTER(ctypes.c_long)),
+                                                  _dp(r)))
+
+    def save(self, path):
+        self.ctx._check(lib().hr_mlp_save(self.p, path.encode()))
+
+    def load(self, path):
+        self.ctx._check(lib().hr_mlp_load(self.p, path.encode()))

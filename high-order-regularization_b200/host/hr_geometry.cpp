@@ -329,13 +329,21 @@ double mean_curvature(const Spheroid& S, const double axes[3], const double* x) 
   return c * (a_sq + temp) / (2.0 * a * sqrt(temp * temp * temp));
 }
 
-// surfc_force: 2S/surface.cpp:530-559 (gamma = 1 + z^2, f = 2 H gamma n - grad_s gamma)
+// surfc_force: 2S/surface.cpp:530-559 (gamma = 1 + z^2, f = 2 H gamma n - grad_s gamma).
+// body_z: z is the body-frame coordinate (row 2 of the un-rotation), so the
+// tension field turns with the surface; otherwise the reference's z - centre_z.
 void surface_force(const Spheroid& S, const double axes[3], const double* x0, const double* n0,
-                   double* f) {
+                   double* f, bool body_z = false) {
   double H = mean_curvature(S, axes, x0);
   double zz = x0[2] - S.ctr[2];
-  double gamma = 1.0 + zz * zz;
   double Dgx = 0.0, Dgy = 0.0, Dgz = 2.0 * zz;
+  if (body_z && S.rotated) {
+    zz = S.R[2][0] * (x0[0] - S.ctr[0]) + S.R[2][1] * (x0[1] - S.ctr[1]) + S.R[2][2] * (x0[2] - S.ctr[2]);
+    Dgx = 2.0 * zz * S.R[2][0];
+    Dgy = 2.0 * zz * S.R[2][1];
+    Dgz = 2.0 * zz * S.R[2][2];
+  }
+  double gamma = 1.0 + zz * zz;
   double Dgn = Dgx * n0[0] + Dgy * n0[1] + Dgz * n0[2];
   double sg0 = Dgx - Dgn * n0[0], sg1 = Dgy - Dgn * n0[1], sg2 = Dgz - Dgn * n0[2];
   gamma *= 2.0 * H;
@@ -504,7 +512,7 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
       G->area[s][i] = P[s][i].area;
       G->plane[s][i] = P[s][i].plane;
       // set_surface_force (2S/main.cpp:1050-1059)
-      surface_force(cen[s], prm->axes, P[s][i].x, P[s][i].n, &G->f[s][3 * i]);
+      surface_force(cen[s], prm->axes, P[s][i].x, P[s][i].n, &G->f[s][3 * i], prm->tension_body != 0);
     }
   }
   // Compute_nearest_data: 2S/surface.cpp:450-526 (targets of set t vs surface 1-t)
@@ -543,7 +551,7 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
         G->nrst[t][i] = 0;
         continue;
       }
-      surface_force(S, prm->axes, x0, n0, &G->f0[t][3 * i]);
+      surface_force(S, prm->axes, x0, n0, &G->f0[t][3 * i], prm->tension_body != 0);
     }
   }
   *out = G.release();

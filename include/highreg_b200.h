@@ -35,7 +35,7 @@ extern "C" {
 #define HR_DIRECT 0 /* all-pairs sums: eval_Stokes_*_{on,off}Surf (2S/stokeslets.cpp, 2S/stresslets.cpp) */
 #define HR_TREE 1   /* KITC treecode: eval_Stokes_*_tree (2S/KITC.cpp:1389-1830) */
 #define HR_FP64 0   /* all pairs in FP64 */
-#define HR_MIXED 1  /* far pairs / proxy interactions in FP32 with FP64 per-target accumulation */
+#define HR_MIXED 1  /* pairs with r > 3 delta and proxy interactions in FP32, FP64 per-target accumulation */
 
 typedef struct hr_ctx hr_ctx;
 
@@ -188,6 +188,11 @@ typedef struct {
   int precision;       /* HR_FP64, or HR_MIXED: relaxed-precision matvecs */
   int use_guess;       /* 1: x holds an initial guess on input */
   int true_residual;   /* 1: check ||b - A x|| / ||b|| with an FP64 matvec at the end */
+  /* HR_MIXED only: relative accuracy assumed for a mixed-precision matvec
+   * (0 = 1e-7; the measured max-norm relative error is 3.5e-8). Relaxed GMRES (Simoncini & Szyld 2003) switches iteration k
+   * to mixed matvecs once ||r_k|| / ||b|| <= tol / mixed_accuracy; a final
+   * FP64 true residual above 10 tol sends the solve back to FP64 matvecs. */
+  double mixed_accuracy;
 } hr_gmres_opts;
 
 typedef struct {
@@ -250,6 +255,9 @@ typedef struct {
   double unrot[2][9];   /* row-major "un-rotation" R: body coordinates = R (x - centre) */
   int rotated[2];       /* 1: the level set uses unrot (the reference's rotated flag) */
   double kappa0, q;     /* delta = kappa0 (1/64)^(1-q) h^q */
+  int tension_body;     /* surface tension gamma = 1 + z^2: 0 = z - centre_z (the reference),
+                           1 = the body-frame z of unrot (the same for an unrotated surface or
+                           a rotation about z, as in the reference's scene) */
 } hr_geom2s_params;
 
 typedef struct hr_geom2s hr_geom2s;
@@ -260,6 +268,83 @@ int hr_geom2s_generate(const hr_geom2s_params* p, int N, hr_geom2s** out);
  * f = 2 H gamma n - grad_s gamma, gamma = 1 + z^2, at every quadrature point. */
 int hr_geom2s_view(const hr_geom2s* g, hr_scene2s* scene, const double** force);
 void hr_geom2s_destroy(hr_geom2s* g);
+
+/* ------------------------------------------------- learned warm start */
+/* No counterpart in the reference (its GMRES starts from zero,
+ * 2S/main.cpp:1067-1075). A pointwise MLP maps local geometry to an initial
+ * guess for the two-surface solve; hr_plan2s_solve with use_guess = 1 takes
+ * it and falls back to the zero guess when ||b - A x0|| > ||b||, so the
+ * converged answer is the zero-guess method's. */
+
+/* Seeded two-surface instance: the reference's spheroid (axes 1, .5, .5) at
+ * the origin, a second one rotated by a uniform random rotation (Shoemake
+ * quaternion) and offset along a uniform random direction so that the solids
+ * are `gap` apart, gap uniform in [0.02, 0.3] x 2 (the major diameter), and a
+ * background rigid motion u(x) = U + Omega x (x - xmid) with |U| = |Omega| = 1.
+ * Instance `index` is the index-th draw of std::mt19937_64(seed). The
+ * right-hand side of an instance is hr_plan2s_rhs(force) + 2/3 u: rigid
+ * motions satisfy (I - 2/3 D) u = 2/3 u, so its solution is u plus the
+ * response to the interfacial force. */
+typedef struct {
+  hr_geom2s_params geom; /* for hr_geom2s_generate */
+  double U[3], Omega[3], xmid[3];
+  double gap;            /* distance between the two solids */
+} hr_warm_instance;
+int hr_warm_instance_make(unsigned long long seed, int index, hr_warm_instance* out);
+/* u(x) at n points (3 doubles each). */
+int hr_warm_imposed_velocity(const hr_warm_instance* w, const double* xyz, int n, double* u);
+
+#define HR_WARM_NFEAT 12
+/* Features of every quadrature point, surface 0 then surface 1 (the GMRES
+ * vector's order), 12 floats each: unit normal (3), principal curvatures
+ * k1 >= k2 (2), distance to the other solid (1), unit direction to its nearest
+ * point (3), imposed velocity u(x) (3). Vectors are in the body frame of the
+ * point's own surface (v_body = R v, R = geom.unrot of that surface, or the
+ * identity when it is not rotated). u_imposed (optional): u(x) in FP64, world
+ * frame, 3 per point. */
+int hr_warm_features(const hr_scene2s* scene, const hr_warm_instance* w, float* feat, double* u_imposed);
+/* The two body frames (18 doubles: R of surface 0, R of surface 1, row-major,
+ * v_body = R v_world) for hr_mlp_infer_frames. */
+int hr_warm_frames(const hr_warm_instance* w, double* rot);
+
+/* The network 12 -> 64 -> 64 -> 64 -> 3 (SiLU, FP32), trained and applied
+ * on the device. Parameters: W1[12][64] b1[64] W2[64][64] b2[64] W3[64][64]
+ * b3[64] W4[64][3] b4[3] (9347 floats), W[i][j] = input i to output j. */
+typedef struct hr_mlp hr_mlp;
+int hr_mlp_nparams(void);
+/* Glorot-uniform weights from `seed`, zero biases, identity normalization. */
+int hr_mlp_create(hr_ctx* ctx, unsigned long long seed, hr_mlp** out);
+void hr_mlp_destroy(hr_mlp* m);
+/* Input normalization x' = (x - mean) / std (12 each) and output scale. */
+int hr_mlp_set_normalization(hr_mlp* m, const float* mean, const float* stdv, float out_scale);
+int hr_mlp_get_params(hr_mlp* m, float* host);
+/* Also resets the Adam moments and step count. */
+int hr_mlp_set_params(hr_mlp* m, const float* host);
+/* One Adam step (lr, beta 0.9 / 0.999, eps 1e-8) on the mean squared error
+ * of MLP(X) against T / out_scale over a batch of `batch` samples of the
+ * device arrays X (n x 12) and T (n x 3): random = 1 draws the batch by a
+ * hash of (seed, step, slot), random = 0 takes samples 0..batch-1. lr = 0
+ * computes the gradient only. loss (optional): the batch's mean loss. */
+int hr_mlp_train_step(hr_mlp* m, const float* X_dev, const float* T_dev, long n, int batch, int random,
+                      unsigned long long seed, float lr, double* loss);
+/* Gradient of the mean loss over samples 0..batch-1, to the host. */
+int hr_mlp_gradient(hr_mlp* m, const float* X_dev, const float* T_dev, int batch, float* grad_host,
+                    double* loss);
+/* out[s] = base[s] + out_scale * MLP(X[s]) (FP64, 3 per sample; base may be
+ * NULL); raw (optional, FP32): the network output before scaling. */
+int hr_mlp_infer(hr_mlp* m, const float* X_dev, long n, const double* base_dev, double* out_dev,
+                 float* raw_dev);
+/* The same with the output in body frames: samples frame_start[f] ..
+ * frame_start[f+1]-1 (host array, nframes + 1 entries, nframes <= 8) use
+ * rot[9 f ..] (host, row-major, v_body = R v_world) and get
+ * out[s] = base[s] + out_scale * R^T MLP(X[s]). */
+int hr_mlp_infer_frames(hr_mlp* m, const float* X_dev, long n, const double* base_dev, double* out_dev,
+                        int nframes, const long* frame_start, const double* rot);
+/* Weights file: "HRMLP001", layer widths (5 int32), 12 means, 12 stds,
+ * out_scale, 9347 FP32 parameters, FNV-1a 64-bit checksum of the rest. A
+ * file with another header, shape or checksum is rejected (HR_ERR_ARG). */
+int hr_mlp_save(hr_mlp* m, const char* path);
+int hr_mlp_load(hr_mlp* m, const char* path);
 
 /* -------------------------------------------------- measured FP64 peak */
 /* Runs an FP64 FMA throughput loop on the device; returns FLOP/s. */
