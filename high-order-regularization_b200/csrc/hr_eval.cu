@@ -28,6 +28,29 @@ namespace hr {
 
 namespace {
 
+#define HR_SMOOTH_STORAGE __device__ const
+#include "hr_smoothing_tables.inc"
+
+// On-surface smoothing factors without erf / exp / rsqrt: for r <= 8 delta,
+// s1 = G1(s) / delta, s2 = G2(s) / delta^3, s3 = G3(s) / delta^5 with
+// s = r^2 / delta^2, each G a piecewise polynomial (64 pieces uniform in
+// r/delta, degree 11 in s - centre) fitted in 80-digit arithmetic to the
+// reference's formulas (2S/utilities.cpp:211-254, :292-323) with ~1e-16
+// relative error; G(0) is the reference's r -> 0 value. The table of a kernel
+// family is staged in shared memory once per CTA.
+constexpr int kSmoothN = HR_SMOOTH_PIECES * (HR_SMOOTH_DEG + 2);
+
+__device__ __forceinline__ double smooth_eval(const double* __restrict__ tab, double s) {
+  int i = (int)(sqrtf((float)s) * (HR_SMOOTH_PIECES / 8.0f));
+  i = min(max(i, 0), HR_SMOOTH_PIECES - 1);
+  const double* p = tab + i * (HR_SMOOTH_DEG + 2);
+  const double t = s - p[0];
+  double v = p[HR_SMOOTH_DEG + 1];
+#pragma unroll
+  for (int k = HR_SMOOTH_DEG; k >= 1; k--) v = fma(v, t, p[k]);
+  return v;
+}
+
 constexpr int kNT = 256;         // sources per shared-memory tile
 constexpr int kSmem = 10 * kNT;  // doubles: 10 SoA arrays of a source tile
 constexpr int kMaxP1 = 16;
@@ -128,7 +151,8 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
 // One FP64 pair; returns true if the smoothed (erf) branch was taken.
 template <int KIND>
 __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, const Tgt& S,
-                                       const Reg& g, double& a0, double& a1, double& a2) {
+                                       const Reg& g, const double* __restrict__ stab, double& a0,
+                                       double& a1, double& a2) {
   const double* X = sm;
   const double* Y = sm + kNT;
   const double* Z = sm + 2 * kNT;
@@ -141,18 +165,41 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
   const double* QZ = sm + 9 * kNT;
   const double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
   const double r2 = dx * dx + dy * dy + dz * dz;
-  const double rinv = rsqrt(r2);
+  constexpr bool kTab = (KIND == K_SL_ON || KIND == K_DL_ON);  // tabulated smoothing, rsqrt only if r > 8 delta
+  const double rinv = kTab ? 0.0 : rsqrt(r2);
   bool reg = false;
-  if (KIND == K_SL_ON || ((KIND == K_SL_OFF || KIND == K_E2G_SL7) && S.near)) {
-    // Call_Ds_SL_onSurf / Call_Ds_SL regularized branch / stokes_SL_7ord
+  if (KIND == K_SL_ON) {
+    // Call_Ds_SL_onSurf (2S/KITC.cpp:807-846) with Stokes_SL_7ord_onSurf (2S/utilities.cpp:211)
     const double area = A[j];
     const double fx = QX[j] - S.f0n0 * NX[j];
     const double fy = QY[j] - S.f0n0 * NY[j];
     const double fz = QZ[j] - S.f0n0 * NZ[j];
     const double fdd = fx * dx + fy * dy + fz * dz;
     double H1, H2;
-    if (KIND == K_SL_ON) reg = sl_7ord_onsurf(r2, rinv, g, H1, H2);
-    else reg = sl_7ord(r2, rinv, g, S.c, H1, H2);
+    if (r2 > g.d64) {
+      const double ri = rsqrt(r2);
+      H1 = ri;
+      H2 = ri * ri * ri;
+    } else {
+      const double sq = r2 * g.inv_d2;
+      H1 = smooth_eval(stab, sq) * g.inv_d;
+      H2 = smooth_eval(stab + kSmoothN, sq) * g.inv_d3;
+      reg = r2 >= g.r0sq;
+    }
+    H1 *= area;
+    H2 *= area * fdd;
+    a0 += fx * H1 + dx * H2;
+    a1 += fy * H1 + dy * H2;
+    a2 += fz * H1 + dz * H2;
+  } else if ((KIND == K_SL_OFF || KIND == K_E2G_SL7) && S.near) {
+    // Call_Ds_SL regularized branch (2S/KITC.cpp:847) / stokes_SL_7ord (E2G/stokes.cpp:53)
+    const double area = A[j];
+    const double fx = QX[j] - S.f0n0 * NX[j];
+    const double fy = QY[j] - S.f0n0 * NY[j];
+    const double fz = QZ[j] - S.f0n0 * NZ[j];
+    const double fdd = fx * dx + fy * dy + fz * dz;
+    double H1, H2;
+    reg = sl_7ord(r2, rinv, g, S.c, H1, H2);
     H1 *= area;
     H2 *= area * fdd;
     a0 += fx * H1 + dx * H2;
@@ -175,7 +222,13 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     const double gdd = gx * dx + gy * dy + gz * dz;
     const double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
     double H3;
-    reg = dl_7ord_onsurf(r2, rinv, g, H3);
+    if (r2 > g.d64) {
+      const double ri = rsqrt(r2), ri2 = ri * ri;
+      H3 = ri2 * ri2 * ri;
+    } else {
+      H3 = smooth_eval(stab, r2 * g.inv_d2) * g.inv_d5;
+      reg = r2 >= g.r0sq;
+    }
     const double kernel = ndd * gdd * H3 * A[j];
     a0 += dx * kernel;
     a1 += dy * kernel;
@@ -510,7 +563,7 @@ __device__ __forceinline__ void proxies32(const float* __restrict__ sf, int PT, 
 template <int KIND, bool MIXED>
 __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
                                          const Seg* __restrict__ segs, double* sm, float* sf,
-                                         double* cheb, float* chebf) {
+                                         double* cheb, float* chebf, const double* stab) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int blk = it.blk;
   const int k = blk * kTB + tid;
@@ -592,7 +645,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
               for (int j = j0; j < j1; j++) {
                 const float dx = F.px - sf[j], dy = F.py - sf[kNT + j], dz = F.pz - sf[2 * kNT + j];
                 if (dx * dx + dy * dy + dz * dz > cut2f) cr += pair32r<KIND>(sf, j, F, gf, p0, p1, p2);
-                else cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
+                else cr += pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
               }
               a0 += (double)p0;
               a1 += (double)p1;
@@ -603,7 +656,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           } else {
             unsigned cr = 0;
 #pragma unroll 2
-            for (int j = 0; j < cnt; j++) cr += pair64<KIND>(sm, j, S, g, a0, a1, a2);
+            for (int j = 0; j < cnt; j++) cr += pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
             if (S.near) {
               creg += cr;
               cplain += cnt - cr;
@@ -682,22 +735,32 @@ __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict
   __shared__ double cheb[3 * kMaxP1];
   __shared__ float chebf[3 * kMaxP1];
   __shared__ EvalTask sT;
+  // smoothing tables: G1, G2 for the Stokeslet family, G3 for the stresslet family
+  __shared__ double stab[FAM == F_SL ? 2 * kSmoothN : (FAM == F_DL ? kSmoothN : 1)];
   const BlockRef it = items[blockIdx.x];
   if (threadIdx.x == 0) sT = tasks[it.task];
+  if (FAM == F_SL) {
+    for (int i = threadIdx.x; i < kSmoothN; i += blockDim.x) {
+      stab[i] = kSmoothG1[i];
+      stab[kSmoothN + i] = kSmoothG2[i];
+    }
+  } else if (FAM == F_DL) {
+    for (int i = threadIdx.x; i < kSmoothN; i += blockDim.x) stab[i] = kSmoothG3[i];
+  }
   __syncthreads();
   const int kind = sT.kind;
   if (FAM == F_SL) {
-    if (kind == K_SL_ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
-    else run_item<K_SL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
+    if (kind == K_SL_ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
+    else run_item<K_SL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
   } else if (FAM == F_DL) {
-    if (kind == K_DL_ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
-    else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf);
+    if (kind == K_DL_ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
+    else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
   } else {
     switch (kind) {
-      case K_E2G_SL_AWAY: run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
-      case K_E2G_P_AWAY: run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
-      case K_E2G_SL7: run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
-      default: run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf); break;
+      case K_E2G_SL_AWAY: run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
+      case K_E2G_P_AWAY: run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
+      case K_E2G_SL7: run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
+      default: run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
     }
   }
 }

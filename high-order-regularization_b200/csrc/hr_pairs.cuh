@@ -28,6 +28,7 @@ struct Coef {
 // Per-target constants of the regularized kernels.
 struct Reg {
   double d, inv_d, d64, r0sq;  // delta, 1/delta, 64 delta^2, (1e-14)^2
+  double inv_d2, inv_d3, inv_d5;
 };
 
 __device__ __forceinline__ Reg make_reg(double d) {
@@ -36,6 +37,9 @@ __device__ __forceinline__ Reg make_reg(double d) {
   g.inv_d = 1.0 / d;
   g.d64 = 64.0 * d * d;
   g.r0sq = 1e-28;
+  g.inv_d2 = g.inv_d * g.inv_d;
+  g.inv_d3 = g.inv_d2 * g.inv_d;
+  g.inv_d5 = g.inv_d3 * g.inv_d2;
   return g;
 }
 
