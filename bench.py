@@ -194,6 +194,65 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def warm_guess_fn(ctx, geo, dev):
+    """The learned warm start for the bench's scene (the reference's default
+    two-spheroid geometry, no imposed motion): returns a function that writes
+    the guess into a device vector, and the host time of the features."""
+    import numpy as np
+    import torch
+
+    import highreg
+    import warmstart
+
+    if not os.path.exists(warmstart.DEFAULT_WEIGHTS):
+        return None, None
+    w = highreg.WarmInstance()
+    w.geom = highreg.Geometry2S.default_params()
+    for k in range(3):
+        w.xmid[k] = 0.5 * (geo["ctr0"][k] + geo["ctr1"][k])
+    t0 = time.perf_counter()
+    feat, uimp = highreg.warm_features(geo, w)
+    feat_s = time.perf_counter() - t0
+    rot = highreg.warm_frames(w)
+    n0 = len(geo["area0"])
+    starts = [0, n0, feat.shape[0]]
+    X = torch.from_numpy(feat).to(dev)
+    base = torch.from_numpy(uimp).to(dev)
+    mlp = highreg.MLP(ctx, 0)
+    mlp.load(warmstart.DEFAULT_WEIGHTS)
+
+    def fn(x):
+        mlp.infer_frames(X, x, base, starts, rot)
+
+    fn.keep = (X, base, mlp)
+    return fn, feat_s
+
+
+def timed_solves(plan, stream, flush, f1, f2, b, x, prec, steps, guess=None):
+    """steps x (L2 flush; RHS + optional guess + GMRES), CUDA events on the plan's stream."""
+    import torch
+
+    times, reps = [], []
+    for _ in range(steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plan.rhs_dev(f1, f2, b)
+        if guess is not None:
+            guess(x)
+        rep = plan.solve_dev(b, x, use_guess=guess is not None, restart=RESTART, tol=TOL, precision=prec)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        reps.append(rep)
+    r = reps[-1]
+    return {"ms_per_step": sum(times) / len(times), "gmres_iterations": r["iterations"],
+            "matvecs_fp64": r["matvecs_fp64"], "matvecs_mixed": r["matvecs_mixed"], "residual": r["residual"],
+            "true_residual": r["true_residual"], "guess_rejected": r["guess_rejected"]}
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -244,6 +303,21 @@ def run_ours(args, rank, world, local_rank):
     launches = ctx.launches - l0
     clocks = clk.stop()
     barrier(world)
+
+    # the metric's comparison on the same workload and protocol: plain FP64,
+    # mixed precision, and mixed precision with the learned warm start
+    variants = {}
+    for name, pr in (("fp64", highreg.HR_FP64), ("mixed", highreg.HR_MIXED)):
+        variants[name] = timed_solves(plan, stream, flush, f1, f2, b, x, pr, args.steps)
+    guess, feat_s = warm_guess_fn(ctx, geo, dev)
+    if guess is not None:
+        timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, guess)
+        v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, args.steps, guess)
+        v["features_host_ms"] = 1e3 * feat_s
+        variants["mixed_warm"] = v
+    for v in variants.values():
+        v["speedup_vs_fp64"] = variants["fp64"]["ms_per_step"] / v["ms_per_step"]
+    del guess  # releases the network before the context goes
     t_local = sum(times) / 1e3
     it = reps[-1]["iterations"]
     mv_per_step = reps[-1]["matvecs_fp64"] + reps[-1]["matvecs_mixed"]
@@ -259,13 +333,15 @@ def run_ours(args, rank, world, local_rank):
     moment_flops = 2.0 * 12 * w_mv["moment_terms"]
     fl_launch = w_mv["flops"] - moment_flops
     peak = ctx.fp64_peak()
+    peak32 = ctx.fp32_peak()
     achieved = fl_launch / (ms_dl * 1e-3)
     roofline = {"bound": "fp64", "kernel": "eval_kernel<F_DL> (stresslet batch, one launch per matvec)",
                 "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                 "frac": achieved / peak, "traffic": None,
                 "flops_per_launch": fl_launch, "ms_per_launch": ms_dl,
                 "ms_per_launch_mixed_precision": ms_dl_mixed,
-                "peak_source": "measured FP64 FMA loop (hr_measure_fp64_peak) on this GPU"}
+                "peak_source": "measured FP64 FMA loop (hr_measure_fp64_peak) on this GPU",
+                "peak_fp32": peak32 / 1e12}
 
     # end to end through the C ABI with host buffers: scene upload + plan
     # (trees, interaction lists, stencils) + RHS + solve + solution read back
@@ -292,7 +368,7 @@ def run_ours(args, rank, world, local_rank):
                 _, dt = cpu_reference_matvec(None)
                 cpu = {"value": pairs_of(w_mv) / dt, "unit": "pairs/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
                        "kind": "reference",
-                       "sample": "one reference operator application (solve_IE_1step, h=1/64, P=6, N0=2000), %.1f s" % dt}
+                       "sample": "one reference operator application (solve_IE_1step, h=1/%d, P=%d, N0=%d), %.1f s" % (H_INV, P, N0, dt)}
             except Exception as e:  # reference build absent
                 cpu = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
                        "sample": "unavailable: %s" % e}
@@ -301,19 +377,116 @@ def run_ours(args, rank, world, local_rank):
                 "warmup": max(3, args.warmup), "ms_per_step": 1e3 * t_max / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (the reference's two-spheroid geometry generated in-process)",
-                "config": {"workload": "two-surface solve h=1/%d (n=%d), KITC P=6 N0=2000 theta=0.6, GMRES restart 50 tol 1e-10, %s" % (H_INV, n, args.precision),
+                "config": {"workload": "two-surface solve h=1/%d (n=%d), KITC P=%d N0=%d theta=0.6, GMRES restart 50 tol 1e-10, %s" % (H_INV, n, P, N0, args.precision),
                            "global_batch": world, "parallelism": "replicas" if world > 1 else "single",
                            "l2": "flushed (256 MB write) before each timed step",
                            "gmres_iterations": it, "matvecs_per_step": mv_per_step,
                            "pairs_per_step": pairs_step, "solve_seconds": t_max / args.steps,
                            "final_residual": reps[-1]["residual"], "true_residual": reps[-1]["true_residual"],
-                           "precision": args.precision, "work_matvec": w_mv, "work_rhs": w_rhs},
+                           "precision": args.precision, "work_matvec": w_mv, "work_rhs": w_rhs,
+                           "variants": variants},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches}
         print(json.dumps(line))
     plan.close()
     ctx.close()
     return line
+
+
+def run_e2g(args, rank, world, local_rank):
+    """Extend-to-grid workload (translating spheroid, h = 3/N): the four
+    boundary sums and the four Poisson extensions on the device, run in FP64,
+    mixed precision (FP32 beyond 3 delta) and all-pairs FP32, each with its
+    error norms against the FP64 grids and against the exact solution."""
+    import numpy as np
+    import torch
+
+    import highreg
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = highreg.Context(local_rank)
+    t0 = time.perf_counter()
+    e = highreg.E2G(ctx, args.N)
+    setup_s = time.perf_counter() - t0
+    info = e.info
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    l0 = ctx.launches
+    clk = ClockSampler(local_rank)
+    variants = {}
+    for name, prec in (("fp64", highreg.HR_FP64), ("mixed", highreg.HR_MIXED), ("fp32", highreg.HR_FP32)):
+        for _ in range(max(3, args.warmup)):
+            e.run(prec)
+        if name == "fp64":
+            clk.start()
+            l0 = ctx.launches
+        reps = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            reps.append(e.run(prec))
+        if name == "fp64":
+            launches = ctx.launches - l0
+            clocks = clk.stop()
+            e.snapshot()
+        err = e.error_norms()
+        v = {k: 1e3 * statistics.mean(r[k] for r in reps) for k in ("seconds_sums", "seconds_poisson", "seconds_total")}
+        v = {"ms_sums": v["seconds_sums"], "ms_poisson": v["seconds_poisson"], "ms_total": v["seconds_total"]}
+        v.update(err)
+        variants[name] = v
+    for v in variants.values():
+        v["speedup_sums_vs_fp64"] = variants["fp64"]["ms_sums"] / v["ms_sums"]
+    pairs = info["pairs"]
+    t_sums = max_over_ranks(variants["fp64"]["ms_sums"] * 1e-3, world)
+    # end to end through the C ABI: host set-up, sums, Poisson solves, grids read back
+    t0 = time.perf_counter()
+    e2 = highreg.E2G(ctx, args.N)
+    e2.run()
+    ug = e2.get(3)
+    e2e_s = time.perf_counter() - t0
+    e2.close()
+    M3 = (args.N + 1) ** 3
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline and args.N <= 96:
+            try:
+                sys.path.insert(0, os.path.join(ROOT, "oracle"))
+                from oracle import RefE2G
+
+                os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+                R = RefE2G()
+                R.setup(args.N)
+                t1 = time.perf_counter()
+                R.eval_p_faces()
+                R.eval_u_faces()
+                dt = time.perf_counter() - t1
+                face_pairs = 2 * info["n_face"] * info["nq"]
+                cpu = {"value": face_pairs / dt, "unit": "pairs/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+                       "kind": "reference",
+                       "sample": "the reference's face sums (stokes_pressure_away, stokes_SL_away) at N=%d, %.1f s"
+                                 % (args.N, dt)}
+            except Exception as ex:
+                cpu = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
+                       "sample": "unavailable: %s" % ex}
+        line = {"metric": "extend-to-grid boundary sums; pairs/s", "value": sum_over_ranks(pairs, world) / t_sums,
+                "unit": "pairs/s", "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup),
+                "ms_per_step": variants["fp64"]["ms_total"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (the reference's translating spheroid generated in-process)",
+                "config": {"workload": "extend-to-grid N=%d (h=3/%d): %d quadrature points, %d band + %d face targets, "
+                                       "4 sums + 4 DST Poisson solves on %d^3" % (args.N, args.N, info["nq"],
+                                                                                  info["n_band"], info["n_face"],
+                                                                                  args.N - 1),
+                           "pairs_per_step": pairs, "host_setup_seconds": setup_s,
+                           "l2": "flushed (256 MB write) before each timed step", "variants": variants},
+                "cpu_baseline": cpu,
+                "e2e": {"value": pairs / e2e_s, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": int(8 * 3 * M3), "seconds_per_step": e2e_s,
+                        "note": "host set-up (quadrature, band tagging) + sums + Poisson + extended u read back"},
+                "clocks": clocks, "gpu_launches": launches}
+        print(json.dumps(line))
+    e.close()
+    ctx.close()
 
 
 def main():
@@ -325,9 +498,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--h", type=int, default=64, help="1/h of the workload (64 is the benchmark)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--P", type=int, default=6, help="treecode degree (6 with h=1/64; 10 with h=1/256)")
+    ap.add_argument("--N0", type=int, default=2000, help="treecode leaf size (2000 with h=1/64; 8000 with h=1/256)")
+    ap.add_argument("--workload", default="2s", choices=["2s", "e2g"],
+                    help="2s: the two-surface solve (the benchmark); e2g: the extend-to-grid pipeline")
+    ap.add_argument("--N", type=int, default=96, help="extend-to-grid grid size (96 or 384)")
     args = ap.parse_args()
-    global H_INV
-    H_INV = args.h
+    global H_INV, P, N0
+    H_INV, P, N0 = args.h, args.P, args.N0
     rank, world, local_rank = dist_info()
     if world > 1:
         import datetime
@@ -340,6 +518,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.workload == "e2g":
+            run_e2g(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -281,6 +281,20 @@ __global__ void fma_peak_kernel(double* out, int iters) {
   if (s == 12345.678) out[0] = s;  // keeps the loop alive
 }
 
+// FP32 counterpart: 16 independent FMA chains per thread.
+__global__ void fma_peak32_kernel(float* out, int iters) {
+  float a[16];
+  for (int q = 0; q < 16; q++) a[q] = 1.0f + 1e-6f * (threadIdx.x + q);
+  const float m = 0.9999999f, c = 1e-7f;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int q = 0; q < 16; q++) a[q] = fmaf(a[q], m, c);
+  }
+  float s = 0;
+  for (int q = 0; q < 16; q++) s += a[q];
+  if (s == 12345.678f) out[0] = s;  // keeps the loop alive
+}
+
 inline int nblk(long n, int t) { return (int)std::min<long>((n + t - 1) / t, 148L * 16); }
 
 }  // namespace
@@ -363,6 +377,10 @@ void launch_copy(int n, const double* a, double* out, cudaStream_t st) {
 
 void launch_fma_peak(double* out, int iters, int blocks, cudaStream_t st) {
   fma_peak_kernel<<<blocks, 256, 0, st>>>(out, iters);
+}
+
+void launch_fma_peak32(float* out, int iters, int blocks, cudaStream_t st) {
+  fma_peak32_kernel<<<blocks, 256, 0, st>>>(out, iters);
 }
 
 }  // namespace hr

@@ -46,7 +46,7 @@ int guard(hr_ctx* ctx, F&& f) {
 void check_opts(const hr_eval_opts* o) {
   HR_REQUIRE(o, "options missing");
   HR_REQUIRE(o->mode == HR_DIRECT || o->mode == HR_TREE, "mode must be HR_DIRECT or HR_TREE");
-  HR_REQUIRE(o->precision == HR_FP64 || o->precision == HR_MIXED, "unknown precision");
+  HR_REQUIRE(o->precision == HR_FP64 || o->precision == HR_MIXED || o->precision == HR_FP32, "unknown precision");
   if (o->mode == HR_TREE) {
     HR_REQUIRE(o->P >= 1 && o->P <= 15, "P must be in [1, 15]");
     HR_REQUIRE(o->N0 >= 1, "N0 must be >= 1");
@@ -177,7 +177,7 @@ void single_eval(Ctx& C, int kind, const hr_eval_opts* opt, double delta, const 
   }
   EvalTask task = make_task(kind, delta, scale, tree, L, tg, d_out.p);
   task.jump_mode = direct ? 1 : 0;
-  task.mixed = (opt && opt->precision == HR_MIXED) ? 1 : 0;
+  task.mixed = opt ? opt->precision : 0;
   if (on) task.tq = q3.p;
   Batch B;
   B.family = dl ? F_DL : ((kind <= K_DL_OFF) ? F_SL : F_E2G);
@@ -408,7 +408,7 @@ struct hr_plan2s {
   DBuf<double> out_on[2], out_off[2];
   DBuf<double> xin, fin;
   DBuf<unsigned long long> counters;  // 4 per task: reg, near-plain, far-target, proxy
-  Batch dl[2];                         // [0] FP64, [1] mixed
+  Batch dl[3];                         // by precision: [0] FP64, [1] mixed, [2] all FP32
   Batch sl;
   // GMRES work space
   int Vcols = 0;
@@ -422,7 +422,7 @@ void plan_batches(hr_plan2s& P) {
   const bool direct = P.opt.mode == HR_DIRECT;
   P.counters.alloc(4 * 8);
   P.counters.zero(st);
-  for (int prec = 0; prec < 2; prec++) {
+  for (int prec = 0; prec < 3; prec++) {
     Batch& B = P.dl[prec];
     B.family = F_DL;
     B.tasks.clear();
@@ -480,7 +480,7 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
                   P.xin.p + P.off[1 - t], P.tg[t].g0.p, st);
     C.launches++;
   }
-  P.dl[prec ? 1 : 0].launch(C);
+  P.dl[prec].launch(C);
   // set 0: u - on*f - comp*f ; set 1: u - comp*f - on*f   (2S/main.cpp:612-676)
   launch_matvec_combine(3 * P.nq[0], 2.0 / 3.0, P.xin.p + P.off[0], P.out_on[0].p, P.out_off[0].p,
                         y_dev + P.off[0], st);
@@ -523,7 +523,7 @@ double dev_norm(hr_plan2s& P, const double* v) {
 // GMRES with classical Gram-Schmidt and one re-orthogonalisation, Givens
 // rotations on the host, relative residual ||r|| / ||b|| (2S/main.cpp:236-416),
 // restarting from the true residual r = b - A x.
-// HR_MIXED relaxes the matvec precision once the residual is small enough
+// HR_MIXED / HR_FP32 relax the matvec precision once the residual is small enough
 // that the FP32 far-field error cannot matter (inexact-Krylov criterion:
 // matvec relative error <= 0.1 tol / residual), then checks the true
 // residual with an FP64 matvec and keeps iterating in FP64 if needed.
@@ -546,8 +546,8 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
   HR_CHECK_CUDA(cudaEventCreate(&e1));
   HR_CHECK_CUDA(cudaEventRecord(e0, st));
   // default: the mixed matvec's measured max-norm relative error is 3.5e-8
-  const double mixed_eps = o.mixed_accuracy > 0.0 ? o.mixed_accuracy : 1e-7;
-  const double relax = o.precision == HR_MIXED ? o.tol / mixed_eps : -1.0;
+  const double mixed_eps = o.mixed_accuracy > 0.0 ? o.mixed_accuracy : (o.precision == HR_FP32 ? 1e-4 : 1e-7);
+  const double relax = o.precision != HR_FP64 ? o.tol / mixed_eps : -1.0;
   double b_norm = dev_norm(P, b_dev);
   double bscale = b_norm > 1.e-8 ? b_norm : 1.0;
   double* r = P.r.p;
@@ -575,7 +575,7 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
   int iter = 0;
   double error = 1.0;
   int status = HR_OK;
-  bool need_true_check = o.true_residual != 0 || o.precision == HR_MIXED;
+  bool need_true_check = o.true_residual != 0 || o.precision != HR_FP64;
   int fp64_tail = 0;  // after a failed true-residual check, stay in FP64
   for (;;) {
     double r_norm = dev_norm(P, r);
@@ -597,7 +597,7 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
       iter++;
       double* vj = P.V.p + (size_t)j * n;
       double* w = P.V.p + (size_t)(j + 1) * n;
-      int prec = (relax > 0 && !fp64_tail && err_prev <= relax) ? 1 : 0;
+      int prec = (relax > 0 && !fp64_tail && err_prev <= relax) ? o.precision : HR_FP64;
       plan_matvec(P, vj, w, prec);
       if (prec) R.matvecs_mixed++;
       else R.matvecs_fp64++;
@@ -766,7 +766,8 @@ extern "C" int hr_plan2s_matvec_dev(hr_plan2s* plan, const double* x_dev, double
   if (!plan) return HR_ERR_ARG;
   return guard(ctx_of(plan), [&] {
     HR_REQUIRE(x_dev && y_dev, "null vector");
-    plan_matvec(*plan, x_dev, y_dev, precision == HR_MIXED ? 1 : 0);
+    HR_REQUIRE(precision == HR_FP64 || precision == HR_MIXED || precision == HR_FP32, "unknown precision");
+    plan_matvec(*plan, x_dev, y_dev, precision);
   });
 }
 
@@ -910,6 +911,34 @@ extern "C" int hr_measure_fp64_peak(hr_ctx* ctx, double* flops_per_s) {
     cudaEventDestroy(b);
     ctx->c.launches += 2;
     double fl = 2.0 * 8.0 * (double)iters * blocks * 256;
+    *flops_per_s = fl / (ms * 1e-3);
+  });
+}
+
+extern "C" int hr_measure_fp32_peak(hr_ctx* ctx, double* flops_per_s) {
+  if (!ctx || !flops_per_s) return HR_ERR_ARG;
+  return guard(ctx, [&] {
+    HR_CHECK_CUDA(cudaSetDevice(ctx->c.device));
+    cudaStream_t st = ctx->c.stream;
+    DBuf<float> o;
+    o.alloc(1);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->c.device);
+    const int blocks = sms * 8, iters = 1 << 14;
+    launch_fma_peak32(o.p, 256, blocks, st);  // warm-up
+    cudaEvent_t a, b;
+    HR_CHECK_CUDA(cudaEventCreate(&a));
+    HR_CHECK_CUDA(cudaEventCreate(&b));
+    HR_CHECK_CUDA(cudaEventRecord(a, st));
+    launch_fma_peak32(o.p, iters, blocks, st);
+    HR_CHECK_CUDA(cudaEventRecord(b, st));
+    HR_CHECK_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ctx->c.launches += 2;
+    double fl = 2.0 * 16.0 * (double)iters * blocks * 256;
     *flops_per_s = fl / (ms * 1e-3);
   });
 }

@@ -16,7 +16,7 @@ struct EvalTask {
   int P1, Pf;     // treecode degree + 1 and (P+1)^3
   int C;          // moment channels stored per node (6 SL, 12 DL)
   int nt;         // number of targets
-  int mixed;      // 1: far pairs / proxies in FP32 with FP64 accumulation
+  int mixed;      // 0 FP64; 1: pairs beyond 3 delta and proxies in FP32 (FP64 accumulation); 2: all pairs FP32
   int pad;
   double DEL;     // regularization length delta
   double scale;   // final factor of the sum (1/8pi, -6/8pi, ...)
@@ -111,5 +111,6 @@ void launch_copy(int n, const double* a, double* out, cudaStream_t st);
 
 // FP64 FMA peak loop.
 void launch_fma_peak(double* out, int iters, int blocks, cudaStream_t st);
+void launch_fma_peak32(float* out, int iters, int blocks, cudaStream_t st);
 
 }  // namespace hr

@@ -44,6 +44,152 @@ __global__ void scatter_kernel(int n, int comps, const long* __restrict__ gi,
 
 constexpr double kPI = 3.14159265358979323846;
 
+// ---------------------------------------------------------------- error norms
+// The exact solution of the translating prolate spheroid (semi-axes 1, .5, .5,
+// centre (1.5, 1.5, 1.5)): p_exact and SL_exact, E2G/utilities.cpp:294-321 and
+// :360-411, evaluated per grid point on the device.
+__device__ void exact_pu(double xi, double yi, double zi, double& p, double u[3]) {
+  const double x = xi - 1.5, y = yi - 1.5, z = zi - 1.5;
+  const double a_sq = 1.0, b_sq = 0.25;
+  const double r_sq = y * y + z * z;
+  const double c = sqrt(a_sq - b_sq);
+  const double R1 = sqrt((x + c) * (x + c) + r_sq);
+  const double R2 = sqrt((x - c) * (x - c) + r_sq);
+  const double R1c = R1 - (x + c);
+  const double R2c = R2 - (x - c);
+  double B10;
+  if (r_sq < 1.e-14) B10 = (x < 0) ? log((x - c) / (x + c)) : log((x + c) / (x - c));
+  else B10 = log(R2c / R1c);
+  const double B30 = (x + c) / R1 - (x - c) / R2;
+  const double dB1dx = 1.0 / R1 - 1.0 / R2;
+  double dB1dyz = 0.0;
+  if (r_sq > 1.e-14) dB1dyz = 1.0 / R2 / R2c - 1.0 / R1 / R1c;
+  const double dB3dyz = 1.0 / R2 - 1.0 / R1 + x * dB1dyz;
+  const double e = c / 1.0;
+  const double Le = log((1.0 + e) / (1.0 - e));
+  const double a1 = e * e / ((1.0 + e * e) * Le - 2.0 * e);
+  const double b1 = a1 * (1.0 - e * e) / (2.0 * e * e);
+  p = -2.0 * a1 * dB1dx;
+  u[0] = 2.0 * a1 * B10 - a1 * B30 + 2.0 * b1 * ((x - c) / R2 - (x + c) / R1 + B10 + x * dB1dx);
+  const double Er = a1 * (1.0 / R2 - 1.0 / R1) + 2.0 * b1 * dB3dyz;
+  u[1] = Er * y;
+  u[2] = Er * z;
+}
+
+// The grids' values where the reference compares (E2G/main.cpp:236-259, 470-497):
+// the exact solution outside or on the surface, p = 0 and u = (1, 0, 0) inside.
+__device__ void grid_exact(int N, double h, long g, double& p, double u[3]) {
+  const long M = N + 1;
+  const int i = (int)(g / (M * M)), j = (int)((g / M) % M), k = (int)(g % M);
+  const double x = i * h, y = j * h, z = k * h;
+  const double lv = (x - 1.5) * (x - 1.5) + (y - 1.5) * (y - 1.5) / 0.25 + (z - 1.5) * (z - 1.5) / 0.25 - 1.0;
+  if (lv > 0.0 || fabs(lv) < 1e-12) {
+    exact_pu(x, y, z, p, u);
+  } else {
+    p = 0.0;
+    u[0] = 1.0;
+    u[1] = u[2] = 0.0;
+  }
+}
+
+constexpr int kErrBlocks = 148 * 4, kErrThreads = 256, kErrVals = 12;
+
+// Per-block maxima and sums (fixed grid-stride assignment, so the final
+// in-order reduction is deterministic):
+//  0 max|p - pex|  1 sum (p - pex)^2  2 max|u - uex|  3 sum |u - uex|^2
+//  4 max|p - pref| 5 sum (p - pref)^2 6 max|pref|     7 sum pref^2
+//  8 max|u - uref| 9 sum |u - uref|^2 10 max|uref|    11 sum |uref|^2
+__global__ void __launch_bounds__(kErrThreads) grid_errors_kernel(int N, double h, const double* __restrict__ p,
+                                                                  const double* __restrict__ u,
+                                                                  const double* __restrict__ pref,
+                                                                  const double* __restrict__ uref,
+                                                                  double* __restrict__ part) {
+  const long M = N + 1, m3 = M * M * M;
+  double v[kErrVals];
+  for (int q = 0; q < kErrVals; q++) v[q] = 0.0;
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < m3; g += (long)gridDim.x * blockDim.x) {
+    double pe, ue[3];
+    grid_exact(N, h, g, pe, ue);
+    const double uu[3] = {u[g], u[m3 + g], u[2 * m3 + g]};
+    const double dp = fabs(p[g] - pe);
+    const double du2 = (uu[0] - ue[0]) * (uu[0] - ue[0]) + (uu[1] - ue[1]) * (uu[1] - ue[1]) +
+                       (uu[2] - ue[2]) * (uu[2] - ue[2]);
+    v[0] = fmax(v[0], dp);
+    v[1] += dp * dp;
+    v[2] = fmax(v[2], sqrt(du2));
+    v[3] += du2;
+    if (pref) {
+      const double rp = fabs(p[g] - pref[g]);
+      const double r0 = uref[g], r1 = uref[m3 + g], r2 = uref[2 * m3 + g];
+      const double ru2 = (uu[0] - r0) * (uu[0] - r0) + (uu[1] - r1) * (uu[1] - r1) + (uu[2] - r2) * (uu[2] - r2);
+      const double un2 = r0 * r0 + r1 * r1 + r2 * r2;
+      v[4] = fmax(v[4], rp);
+      v[5] += rp * rp;
+      v[6] = fmax(v[6], fabs(pref[g]));
+      v[7] += pref[g] * pref[g];
+      v[8] = fmax(v[8], sqrt(ru2));
+      v[9] += ru2;
+      v[10] = fmax(v[10], sqrt(un2));
+      v[11] += un2;
+    }
+  }
+  __shared__ double red[kErrThreads / 32][kErrVals];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = 0; q < kErrVals; q++) {
+    const bool is_max = (q % 2 == 0);
+    double x = v[q];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, x, off);
+      x = is_max ? fmax(x, y) : x + y;
+    }
+    if (lane == 0) red[warp][q] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < kErrVals) {
+    const int q = threadIdx.x;
+    double x = red[0][q];
+    for (int w = 1; w < kErrThreads / 32; w++) x = (q % 2 == 0) ? fmax(x, red[w][q]) : x + red[w][q];
+    part[(size_t)blockIdx.x * kErrVals + q] = x;
+  }
+}
+
+// Band velocity after the sums vs the exact solution at the band targets
+// (E2G/main.cpp:1359-1405): one thread per target, per-block max and sum.
+__global__ void __launch_bounds__(kErrThreads) band_errors_kernel(int N, double h, int nb, const long* __restrict__ gb,
+                                                                  const double* __restrict__ u,
+                                                                  double* __restrict__ part) {
+  const long M = N + 1, m3 = M * M * M;
+  double mx = 0.0, sq = 0.0;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nb; t += gridDim.x * blockDim.x) {
+    const long g = gb[t];
+    double pe, ue[3];
+    grid_exact(N, h, g, pe, ue);
+    const double d0 = u[g] - ue[0], d1 = u[m3 + g] - ue[1], d2 = u[2 * m3 + g] - ue[2];
+    const double d = d0 * d0 + d1 * d1 + d2 * d2;
+    mx = fmax(mx, sqrt(d));
+    sq += d;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    sq += __shfl_down_sync(0xffffffffu, sq, off);
+  }
+  __shared__ double red[kErrThreads / 32][2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[warp][0] = mx;
+    red[warp][1] = sq;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kErrThreads / 32; w++) {
+      mx = fmax(mx, red[w][0]);
+      sq += red[w][1];
+    }
+    part[2 * blockIdx.x] = mx;
+    part[2 * blockIdx.x + 1] = sq;
+  }
+}
+
 }  // namespace
 
 struct hr_e2g {
@@ -58,7 +204,9 @@ struct hr_e2g {
   DBuf<long> gf, gb;
   DBuf<uint8_t> mband2, mout;
   DBuf<double> p_bi, u_bi, p_ext, u_ext;  // grids
-  Batch batch[2];                         // FP64, mixed
+  DBuf<double> p_ref, u_ref;              // snapshot of the extended grids for comparisons
+  bool have_ref = false;
+  Batch batch[3];                         // by precision: FP64, mixed, all FP32
   long long pairs = 0;
 };
 
@@ -153,7 +301,7 @@ extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
     E->pb.alloc(std::max(1, E->nband));
     E->ub.alloc(3 * (size_t)std::max(1, E->nband));
     const double p_scale = 1.0 / (4.0 * kPI), sl_scale = 1.0 / (8.0 * kPI);
-    for (int prec = 0; prec < 2; prec++) {
+    for (int prec = 0; prec < 3; prec++) {
       Batch& B = E->batch[prec];
       B.family = F_E2G;
       EvalTask a = make_task(K_E2G_P_AWAY, S.delta, p_scale, E->tree, E->Lf, E->tf, E->pf.p);
@@ -227,7 +375,8 @@ extern "C" int hr_e2g_run(hr_e2g* E, int precision, hr_e2g_report* rep) {
     cudaEvent_t ev[4];
     for (auto& e : ev) HR_CHECK_CUDA(cudaEventCreate(&e));
     HR_CHECK_CUDA(cudaEventRecord(ev[0], st));
-    E->batch[precision == HR_MIXED ? 1 : 0].launch(C);
+    HR_REQUIRE(precision == HR_FP64 || precision == HR_MIXED || precision == HR_FP32, "unknown precision");
+    E->batch[precision].launch(C);
     HR_CHECK_CUDA(cudaEventRecord(ev[1], st));
     // grids: p = 0, u = (1, 0, 0) off the evaluated points (E2G/main.cpp:1062, 1234-1236)
     int fb = 148 * 8;
@@ -328,3 +477,75 @@ extern "C" void hr_e2g_destroy(hr_e2g* E) {
 
 extern "C" double hr_e2g_p_exact(double x, double y, double z) { return e2g_setup::p_exact(x, y, z); }
 extern "C" void hr_e2g_u_exact(double x, double y, double z, double* u) { e2g_setup::u_exact(x, y, z, u); }
+
+extern "C" int hr_e2g_snapshot(hr_e2g* E) {
+  if (!E) return HR_ERR_ARG;
+  Ctx& C = E->owner->c;
+  try {
+    const long M = E->S.N + 1, m3 = M * M * M;
+    cudaStream_t st = C.stream;
+    if (!E->have_ref) {
+      E->p_ref.alloc(m3);
+      E->u_ref.alloc(3 * m3);
+    }
+    HR_CHECK_CUDA(cudaMemcpyAsync(E->p_ref.p, E->p_ext.p, sizeof(double) * m3, cudaMemcpyDeviceToDevice, st));
+    HR_CHECK_CUDA(cudaMemcpyAsync(E->u_ref.p, E->u_ext.p, sizeof(double) * 3 * m3, cudaMemcpyDeviceToDevice, st));
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+    E->have_ref = true;
+  } catch (const hr::Error& e) {
+    C.err = e.what();
+    return e.code;
+  }
+  return HR_OK;
+}
+
+extern "C" int hr_e2g_error_norms(hr_e2g* E, hr_e2g_errors* out) {
+  if (!E || !out) return HR_ERR_ARG;
+  Ctx& C = E->owner->c;
+  try {
+    cudaStream_t st = C.stream;
+    const int N = E->S.N;
+    const long M = N + 1, m3 = M * M * M;
+    DBuf<double> part, bpart;
+    part.alloc((size_t)kErrBlocks * kErrVals);
+    bpart.alloc(2 * (size_t)kErrBlocks);
+    grid_errors_kernel<<<kErrBlocks, kErrThreads, 0, st>>>(N, E->S.h, E->p_ext.p, E->u_ext.p,
+                                                           E->have_ref ? E->p_ref.p : nullptr,
+                                                           E->have_ref ? E->u_ref.p : nullptr, part.p);
+    band_errors_kernel<<<kErrBlocks, kErrThreads, 0, st>>>(N, E->S.h, E->nband, E->gb.p, E->u_bi.p, bpart.p);
+    C.launches += 2;
+    HR_CHECK_CUDA(cudaGetLastError());
+    std::vector<double> h((size_t)kErrBlocks * kErrVals), hb(2 * (size_t)kErrBlocks);
+    HR_CHECK_CUDA(cudaMemcpyAsync(h.data(), part.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st));
+    HR_CHECK_CUDA(cudaMemcpyAsync(hb.data(), bpart.p, sizeof(double) * hb.size(), cudaMemcpyDeviceToHost, st));
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+    double v[kErrVals] = {0};
+    double bm = 0.0, bs = 0.0;
+    for (int b = 0; b < kErrBlocks; b++) {
+      for (int q = 0; q < kErrVals; q++) {
+        const double x = h[(size_t)b * kErrVals + q];
+        v[q] = (q % 2 == 0) ? std::max(v[q], x) : v[q] + x;
+      }
+      bm = std::max(bm, hb[2 * b]);
+      bs += hb[2 * b + 1];
+    }
+    out->p_max = v[0];
+    out->p_rms = sqrt(v[1] / (double)m3);
+    out->u_max = v[2];
+    out->u_rms = sqrt(v[3] / (double)m3);
+    out->band_u_max = bm;
+    out->band_u_rms = E->nband > 0 ? sqrt(bs / (double)E->nband) : 0.0;
+    if (E->have_ref) {
+      out->ref_p_max_rel = v[6] > 0 ? v[4] / v[6] : 0.0;
+      out->ref_p_rel_l2 = v[7] > 0 ? sqrt(v[5] / v[7]) : 0.0;
+      out->ref_u_max_rel = v[10] > 0 ? v[8] / v[10] : 0.0;
+      out->ref_u_rel_l2 = v[11] > 0 ? sqrt(v[9] / v[11]) : 0.0;
+    } else {
+      out->ref_p_max_rel = out->ref_p_rel_l2 = out->ref_u_max_rel = out->ref_u_rel_l2 = -1.0;
+    }
+  } catch (const hr::Error& e) {
+    C.err = e.what();
+    return e.code;
+  }
+  return HR_OK;
+}

@@ -576,7 +576,9 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   RegF gf;
   gf.inv_d = (float)g.inv_d;
   gf.d64 = (float)g.d64;
-  const float cut2f = (float)(9.0 * T.DEL * T.DEL);  // (3 delta)^2: FP64 below, FP32 above
+  // FP64 below, FP32 above: (3 delta)^2 in the mixed mode; in the all-FP32 mode
+  // only the r < 1e-14 limits of the reference stay in FP64
+  const float cut2f = T.mixed == 2 ? 1e-28f : (float)(9.0 * T.DEL * T.DEL);
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   unsigned long long creg = 0, cplain = 0, cfar = 0, cprox = 0;
   constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY);

@@ -447,11 +447,9 @@ extern "C" int hr_mlp_create(hr_ctx* ctx, unsigned long long seed, hr_mlp** out)
   return HR_OK;
 }
 
-extern "C" void hr_mlp_destroy(hr_mlp* M) {
-  if (!M) return;
-  cudaStreamSynchronize(M->owner->c.stream);
-  delete M;
-}
+// Frees the network's device buffers (cudaFree waits for work using them);
+// it does not touch the owning context, which may already be gone.
+extern "C" void hr_mlp_destroy(hr_mlp* M) { delete M; }
 
 extern "C" int hr_mlp_set_normalization(hr_mlp* M, const float* mean, const float* stdv, float out_scale) {
   if (!M || !mean || !stdv || !(out_scale > 0)) return HR_ERR_ARG;

@@ -12,6 +12,7 @@ from __future__ import annotations
 
 import ctypes
 import os
+import weakref
 
 import numpy as np
 
@@ -20,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "libhighreg_b200.so")
 
 HR_OK, HR_ERR_ARG, HR_ERR_CUDA, HR_ERR_NAN, HR_ERR_NOT_CONVERGED, HR_ERR_NO_DEVICE, HR_ERR_STATE = range(7)
 HR_DIRECT, HR_TREE = 0, 1
-HR_FP64, HR_MIXED = 0, 1
+HR_FP64, HR_MIXED, HR_FP32 = 0, 1, 2
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -190,9 +191,17 @@ class Context:
         if rc != HR_OK:
             raise HrError(rc, "hr_ctx_create failed (no sm_100 device?)")
         self.p = p
+        self._children = weakref.WeakSet()
+
+    def adopt(self, obj):
+        """Registers an object (plan, pipeline, network) that closes with the context."""
+        self._children.add(obj)
 
     def close(self):
+        """Closes the objects made on this context, then the context itself."""
         if self.p:
+            for obj in list(getattr(self, "_children", ())):
+                obj.close()
             lib().hr_ctx_destroy(self.p)
             self.p = None
 
@@ -317,6 +326,11 @@ class Context:
         self._check(lib().hr_measure_fp64_peak(self.p, ctypes.byref(v)))
         return v.value
 
+    def fp32_peak(self):
+        v = ctypes.c_double()
+        self._check(lib().hr_measure_fp32_peak(self.p, ctypes.byref(v)))
+        return v.value
+
 
 class Geometry2S:
     """The product's two-surface scene generator (host C++)."""
@@ -389,6 +403,7 @@ class Plan2S:
 
     def __init__(self, ctx: Context, geo: dict, **opt):
         self.ctx = ctx
+        ctx.adopt(self)
         self.keep = _Keep()
         sc = scene_struct(self.keep, geo)
         self.opts = eval_opts(**opt)
@@ -399,7 +414,7 @@ class Plan2S:
         self.n1 = len(geo["area0"])
 
     def close(self):
-        if self.p:
+        if getattr(self, "p", None):
             lib().hr_plan2s_destroy(self.p)
             self.p = None
 
@@ -459,6 +474,11 @@ class Plan2S:
         return v.value
 
 
+class E2GErrors(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_double) for k in ("p_max", "p_rms", "u_max", "u_rms", "band_u_max", "band_u_rms",
+                                                "ref_p_max_rel", "ref_p_rel_l2", "ref_u_max_rel", "ref_u_rel_l2")]
+
+
 class E2GInfo(ctypes.Structure):
     _fields_ = [("N", ctypes.c_int), ("L", ctypes.c_double), ("h", ctypes.c_double), ("delta", ctypes.c_double),
                 ("nq", ctypes.c_int), ("n_tagged", ctypes.c_int), ("n_band", ctypes.c_int), ("n_face", ctypes.c_int),
@@ -475,6 +495,7 @@ class E2G:
 
     def __init__(self, ctx: Context, N: int):
         self.ctx = ctx
+        ctx.adopt(self)
         p = ctypes.c_void_p()
         ctx._check(lib().hr_e2g_create(ctx.p, N, ctypes.byref(p)))
         self.p = p
@@ -484,7 +505,7 @@ class E2G:
         self.N = N
 
     def close(self):
-        if self.p:
+        if getattr(self, "p", None):
             lib().hr_e2g_destroy(self.p)
             self.p = None
 
@@ -493,6 +514,15 @@ class E2G:
             self.close()
         except Exception:
             pass
+
+    def snapshot(self):
+        """Keeps the current extended grids as the reference of error_norms."""
+        self.ctx._check(lib().hr_e2g_snapshot(self.p))
+
+    def error_norms(self):
+        e = E2GErrors()
+        self.ctx._check(lib().hr_e2g_error_norms(self.p, ctypes.byref(e)))
+        return {k: getattr(e, k) for k, _ in E2GErrors._fields_}
 
     def run(self, precision=HR_FP64):
         rep = E2GReport()
@@ -582,16 +612,20 @@ class MLP:
 
     def __init__(self, ctx: Context, seed: int = 0):
         self.ctx = ctx
+        ctx.adopt(self)
         L = lib()
         L.hr_mlp_destroy.restype = None
         p = ctypes.c_void_p()
         ctx._check(L.hr_mlp_create(ctx.p, ctypes.c_ulonglong(seed), ctypes.byref(p)))
         self.p = p
 
-    def __del__(self):
+    def close(self):
         if getattr(self, "p", None):
             lib().hr_mlp_destroy(self.p)
             self.p = None
+
+    def __del__(self):
+        self.close()
 
     def set_normalization(self, mean, std, out_scale):
         m = np.ascontiguousarray(mean, np.float32)

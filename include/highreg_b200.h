@@ -36,6 +36,7 @@ extern "C" {
 #define HR_TREE 1   /* KITC treecode: eval_Stokes_*_tree (2S/KITC.cpp:1389-1830) */
 #define HR_FP64 0   /* all pairs in FP64 */
 #define HR_MIXED 1  /* pairs with r > 3 delta and proxy interactions in FP32, FP64 per-target accumulation */
+#define HR_FP32 2   /* every pair in FP32 (the r < 1e-14 limits excepted), FP64 per-target accumulation */
 
 typedef struct hr_ctx hr_ctx;
 
@@ -70,7 +71,7 @@ typedef struct {
   int P;         /* treecode interpolation degree (2S/KITC.h:14) */
   int N0;        /* treecode leaf size (2S/KITC.h:16) */
   double theta;  /* treecode MAC parameter, sq_theta = theta^2 (2S/KITC.h:17) */
-  int precision; /* HR_FP64 or HR_MIXED */
+  int precision; /* HR_FP64, HR_MIXED or HR_FP32 */
 } hr_eval_opts;
 
 /* ---------------------------------------------------------------- context */
@@ -165,6 +166,22 @@ int hr_e2g_get(hr_e2g* e, int which, double* out);
  * (N+1)^3), 2 tagged targets (b, 3 x0, 3 n0, band2) as doubles */
 int hr_e2g_scene(const hr_e2g* e, int which, void* out);
 void hr_e2g_destroy(hr_e2g* e);
+/* Error norms of the last hr_e2g_run, computed on the device: extended p and
+ * u against the exact solution over the whole grid (exact outside or on the
+ * surface, p = 0 and u = (1, 0, 0) inside; the reference's tables,
+ * E2G/main.cpp:236-259, 470-497), the band velocity after the sums against
+ * the exact solution (E2G/main.cpp:1359-1405), and, after hr_e2g_snapshot,
+ * the extended grids against the snapshot: max |x - ref| / max |ref| and
+ * ||x - ref||_2 / ||ref||_2 (-1 without a snapshot). u errors use |u| (the
+ * Euclidean norm of the vector at a point). */
+typedef struct {
+  double p_max, p_rms, u_max, u_rms;
+  double band_u_max, band_u_rms;
+  double ref_p_max_rel, ref_p_rel_l2, ref_u_max_rel, ref_u_rel_l2;
+} hr_e2g_errors;
+/* keeps the current extended p and u grids (device copies) as the comparison reference */
+int hr_e2g_snapshot(hr_e2g* e);
+int hr_e2g_error_norms(hr_e2g* e, hr_e2g_errors* out);
 /* exact translating-spheroid solution (E2G/utilities.cpp:294-411) */
 double hr_e2g_p_exact(double x, double y, double z);
 void hr_e2g_u_exact(double x, double y, double z, double* u);
@@ -185,11 +202,12 @@ typedef struct {
   int restart;         /* GMRES restart length (reference: 15, 2S/main.cpp:213) */
   int max_iter;        /* iteration cap (reference: 100) */
   double tol;          /* relative residual tolerance (reference: 1e-10) */
-  int precision;       /* HR_FP64, or HR_MIXED: relaxed-precision matvecs */
+  int precision;       /* HR_FP64, or HR_MIXED / HR_FP32: relaxed-precision matvecs */
   int use_guess;       /* 1: x holds an initial guess on input */
   int true_residual;   /* 1: check ||b - A x|| / ||b|| with an FP64 matvec at the end */
-  /* HR_MIXED only: relative accuracy assumed for a mixed-precision matvec
-   * (0 = 1e-7; the measured max-norm relative error is 3.5e-8). Relaxed GMRES (Simoncini & Szyld 2003) switches iteration k
+  /* HR_MIXED / HR_FP32: relative accuracy assumed for a reduced-precision
+   * matvec (0 = 1e-7 for HR_MIXED, whose measured max-norm relative error is
+   * 3.5e-8, and 1e-4 for HR_FP32). Relaxed GMRES (Simoncini & Szyld 2003) switches iteration k
    * to mixed matvecs once ||r_k|| / ||b|| <= tol / mixed_accuracy; a final
    * FP64 true residual above 10 tol sends the solve back to FP64 matvecs. */
   double mixed_accuracy;
@@ -349,6 +367,8 @@ int hr_mlp_load(hr_mlp* m, const char* path);
 /* -------------------------------------------------- measured FP64 peak */
 /* Runs an FP64 FMA throughput loop on the device; returns FLOP/s. */
 int hr_measure_fp64_peak(hr_ctx* ctx, double* flops_per_s);
+/* The same with FP32 FMAs (16 independent chains per thread). */
+int hr_measure_fp32_peak(hr_ctx* ctx, double* flops_per_s);
 
 /* -------------------------------------- allocation-free Stokeslet sum */
 /* No counterpart in the reference. The plain Stokeslet sum of

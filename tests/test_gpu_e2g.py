@@ -36,9 +36,14 @@ def test_pipeline_matches_reference(e48, ge2g):
     assert rel_err(e48.get(1), ge2g["u_band"]) < 1e-12
     assert rel_err(e48.get(2), ge2g["p_ext"]) < 1e-11
     assert rel_err(e48.get(3), ge2g["u_ext"]) < 1e-11
-    # mixed precision: face sums in FP32, band sums split by r <= 8 delta
+    # mixed precision: face sums in FP32, band sums split at r = 3 delta
     e48.run(highreg.HR_MIXED)
     assert rel_err(e48.get(3), ge2g["u_ext"]) < 1e-6
+    # every pair in FP32
+    e48.run(highreg.HR_FP32)
+    e32 = rel_err(e48.get(3), ge2g["u_ext"])
+    print("E2G N=48 extended velocity, FP32 pairs vs the reference:", e32)
+    assert e32 < 1e-3
 
 
 def _exact_grids(N, h):
@@ -86,4 +91,21 @@ def test_exact_solution_error_table_h32(ctx):
     be = np.sqrt(np.sum((ub[:, gb] - uex[:, gb]) ** 2, axis=0))
     assert abs(be.max() - 4.2629e-04) / 4.2629e-04 < 1e-3
     assert abs(np.sqrt(np.mean(be ** 2)) - 2.42985e-05) / 2.42985e-05 < 1e-3
+    # the device error norms give the same table
+    d = e.error_norms()
+    assert abs(d["p_max"] - perr.max()) <= 1e-12 * perr.max()
+    assert abs(d["p_rms"] - np.sqrt(np.mean(perr ** 2))) <= 1e-9 * d["p_rms"]
+    assert abs(d["u_max"] - uerr.max()) <= 1e-12 * uerr.max()
+    assert abs(d["u_rms"] - np.sqrt(np.mean(uerr ** 2))) <= 1e-9 * d["u_rms"]
+    assert abs(d["band_u_max"] - be.max()) <= 1e-12 * be.max()
+    assert abs(d["band_u_rms"] - np.sqrt(np.mean(be ** 2))) <= 1e-9 * d["band_u_rms"]
+    assert d["ref_u_rel_l2"] == -1.0
+    # precision variants against the FP64 grids and the exact solution
+    e.snapshot()
+    for prec, tol in ((highreg.HR_MIXED, 1e-7), (highreg.HR_FP32, 1e-3)):
+        e.run(prec)
+        d2 = e.error_norms()
+        print("E2G N=96 precision", prec, d2)
+        assert d2["ref_u_rel_l2"] < tol and d2["ref_p_rel_l2"] < tol
+        assert abs(d2["u_max"] - d["u_max"]) <= 0.05 * d["u_max"]
     e.close()

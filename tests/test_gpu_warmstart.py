@@ -184,3 +184,17 @@ def test_trained_network_improves_the_guess(ctx):
     assert err_guess < 0.5 * err_imposed
     assert w["iterations"] <= z["iterations"] + 1
     assert float(torch.linalg.norm(S.x - xz) / torch.linalg.norm(xz)) < 1e-8
+
+
+def test_closing_the_context_closes_its_objects():
+    """Plans and networks made on a context are released before it, whatever
+    order the caller drops them in."""
+    import warmstart
+
+    c = highreg.Context(0)
+    prob = warmstart.Problem(warmstart.SEED, 450, 12)
+    plan = highreg.Plan2S(c, prob.geo, mode=highreg.HR_TREE, P=4, N0=300, theta=0.6)
+    m = highreg.MLP(c, 1)
+    c.close()
+    assert plan.p is None and m.p is None
+    del plan, m
