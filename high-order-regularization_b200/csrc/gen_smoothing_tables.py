@@ -18,7 +18,9 @@ interpolant at DEG + 1 Chebyshev nodes of the piece widened by 1e-3 in lam at
 each end, solved in 80-digit arithmetic (mpmath). The script checks the
 rounded coefficients against the 80-digit function on a dense grid and
 writes the maximum relative error into the generated file (~1e-16 with
-64 pieces of degree 11).
+64 pieces of degree 11). For the FP32 path it also writes float tables with
+pieces uniform in s (so the piece index needs no square root), checked by
+emulating their FP32 evaluation.
 
 Run from this directory: python gen_smoothing_tables.py
 """
@@ -104,6 +106,51 @@ def build(f):
     return out, worst
 
 
+# FP32 tables for the mixed-precision path: NI32 pieces uniform in s (index
+# floor(s * NI32 / 64), no square root), degree DEG32, each piece stored as
+# 8 floats (centre, coefficients of t^0 .. t^5, 0) = two float4.
+NI32 = 128
+DEG32 = 5
+
+
+def piece32(f, i):
+    w = mp.mpf(64) / NI32
+    slo = max(mp.mpf(0), i * w - mp.mpf("0.01"))
+    shi = (i + 1) * w + mp.mpf("0.01")
+    c = (i + mp.mpf(1) / 2) * w
+    half, mid = (shi - slo) / 2, (shi + slo) / 2
+    n = DEG32 + 1
+    ts = [mid + half * mp.cos(mp.pi * (k + mp.mpf(1) / 2) / n) - c for k in range(n)]
+    V = mp.matrix(n, n)
+    for r, t in enumerate(ts):
+        for j in range(n):
+            V[r, j] = t ** j
+    coef = mp.lu_solve(V, mp.matrix([f(t + c) for t in ts]))
+    return [coef[j] for j in range(n)], c
+
+
+def build32(f):
+    """Float pieces and the worst relative error of their FP32 Horner evaluation
+    (emulated with numpy float32) over 21 points per piece."""
+    import numpy as np
+    out, worst = [], 0.0
+    w = 64.0 / NI32
+    for i in range(NI32):
+        coef, c = piece32(f, i)
+        cf = np.array([float(a) for a in coef], np.float32)
+        cc = np.float32(float(c))
+        for k in range(21):
+            sv = np.float32(i * w + w * k / 20.0)
+            t = np.float32(sv - cc)
+            v = cf[-1]
+            for a in cf[-2::-1]:
+                v = np.float32(v * t + a)
+            ex = f(mp.mpf(float(sv)))
+            worst = max(worst, float(abs(mp.mpf(float(v)) - ex) / abs(ex)))
+        out.append([float(cc)] + [float(a) for a in cf] + [0.0] * (6 - DEG32))
+    return out, worst
+
+
 def main():
     lines = ["// Generated by gen_smoothing_tables.py; do not edit.",
              "// Piecewise polynomials G(s), s = (r/delta)^2 in [0, 64], of the on-surface",
@@ -119,6 +166,18 @@ def main():
         lines.append("HR_SMOOTH_STORAGE double kSmooth%s[%d * %d] = {" % (name, NI, DEG + 2))
         for c, cd in tab:
             lines.append("    " + ", ".join(repr(v) for v in [c] + cd) + ",")
+        lines.append("};")
+    lines.append("// FP32 tables: %d pieces uniform in s (width %g), degree %d; per piece 8 floats:"
+                 % (NI32, 64.0 / NI32, DEG32))
+    lines.append("// centre, coefficients of t^0 .. t^%d, 0." % DEG32)
+    lines.append("#define HR_SMOOTH32_PIECES %d" % NI32)
+    for name, f in (("G1", G1), ("G2", G2), ("G3", G3)):
+        tab, worst = build32(f)
+        lines.append("// %s (FP32): max relative error of the FP32 evaluation %.2e" % (name, worst))
+        print(name, "FP32 max rel err", worst)
+        lines.append("HR_SMOOTH_STORAGE float kSmooth32%s[%d * 8] = {" % (name, NI32))
+        for row in tab:
+            lines.append("    " + ", ".join("%.9ef" % v for v in row) + ",")
         lines.append("};")
     with open(os.path.join(HERE, "hr_smoothing_tables.inc"), "w") as fh:
         fh.write("\n".join(lines) + "\n")

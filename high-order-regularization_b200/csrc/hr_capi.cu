@@ -13,8 +13,7 @@ using namespace hr;
 namespace hr {
 // implemented in hr_poisson.cu
 void dst_poisson3d_dev(Ctx& C, int n, double* f_dev);
-void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const uint8_t* out_dev,
-                       const double* p_dev, double* u_dev, int variable);
+
 }  // namespace hr
 
 namespace {
@@ -155,7 +154,7 @@ void single_eval(Ctx& C, int kind, const hr_eval_opts* opt, double delta, const 
   tree.build(*S, P, N0, theta, direct, st);
   DBuf<double> q3;
   q3.upload(dens, 3 * (size_t)S->n, st);
-  tree.set_density(C, q3.p, dl, !direct);
+  tree.set_density(C, q3.p, dl, !direct, opt && opt->precision != HR_FP64);
   std::vector<uint8_t> near =
       (kind == K_SL_OFF || kind == K_DL_OFF) ? near_flags(nt, b, delta) : std::vector<uint8_t>(nt, 1);
   DevTargets tg;
@@ -189,6 +188,7 @@ void single_eval(Ctx& C, int kind, const hr_eval_opts* opt, double delta, const 
   HR_CHECK_CUDA(cudaGetLastError());
   HR_CHECK_CUDA(cudaMemcpyAsync(out, d_out.p, sizeof(double) * odim * nt, cudaMemcpyDeviceToHost, st));
   HR_CHECK_CUDA(cudaStreamSynchronize(st));
+  if (opt && opt->precision != HR_FP64) C.check_tc();
 }
 
 }  // namespace
@@ -473,7 +473,7 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
   const bool tree = P.opt.mode == HR_TREE;
   if (x_dev != P.xin.p)
     HR_CHECK_CUDA(cudaMemcpyAsync(P.xin.p, x_dev, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
-  for (int s = 0; s < 2; s++) P.tree[s].set_density(C, P.xin.p + P.off[s], true, tree);
+  for (int s = 0; s < 2; s++) P.tree[s].set_density(C, P.xin.p + P.off[s], true, tree, prec != HR_FP64);
   for (int t = 0; t < 2; t++) {
     P.tg[t].g0.zero(st);
     launch_interp(P.sten[t].ne, P.sten[t].tgt.p, P.sten[t].idx.p, P.sten[t].pq.p,
@@ -523,10 +523,13 @@ double dev_norm(hr_plan2s& P, const double* v) {
 // GMRES with classical Gram-Schmidt and one re-orthogonalisation, Givens
 // rotations on the host, relative residual ||r|| / ||b|| (2S/main.cpp:236-416),
 // restarting from the true residual r = b - A x.
-// HR_MIXED / HR_FP32 relax the matvec precision once the residual is small enough
-// that the FP32 far-field error cannot matter (inexact-Krylov criterion:
-// matvec relative error <= 0.1 tol / residual), then checks the true
-// residual with an FP64 matvec and keeps iterating in FP64 if needed.
+// HR_MIXED / HR_FP32 solve by iterative refinement with reduced-precision
+// inner GMRES (GMRES-IR): every Krylov matvec is in the reduced precision; a
+// cycle stops once its Arnoldi residual has fallen by eta = 10 x
+// mixed_accuracy (or below tol / 2); the FP64 true residual r = b - A x then
+// starts the next cycle, and the solve ends when that FP64 residual meets
+// tol. A cycle that does not halve the true residual sends the rest of the
+// solve to FP64 matvecs.
 int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double* x_dev,
                hr_gmres_report* rep) {
   Ctx& C = *P.C;
@@ -545,9 +548,10 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
   HR_CHECK_CUDA(cudaEventCreate(&e0));
   HR_CHECK_CUDA(cudaEventCreate(&e1));
   HR_CHECK_CUDA(cudaEventRecord(e0, st));
-  // default: the mixed matvec's measured max-norm relative error is 3.5e-8
-  const double mixed_eps = o.mixed_accuracy > 0.0 ? o.mixed_accuracy : (o.precision == HR_FP32 ? 1e-4 : 1e-7);
-  const double relax = o.precision != HR_FP64 ? o.tol / mixed_eps : -1.0;
+  // default: the mixed matvec's measured max-norm relative error is 2.7e-7
+  const double mixed_eps = o.mixed_accuracy > 0.0 ? o.mixed_accuracy : (o.precision == HR_FP32 ? 1e-6 : 3e-7);
+  const bool refine = o.precision != HR_FP64;
+  const double eta = std::min(0.1, 10.0 * mixed_eps);
   double b_norm = dev_norm(P, b_dev);
   double bscale = b_norm > 1.e-8 ? b_norm : 1.0;
   double* r = P.r.p;
@@ -576,7 +580,7 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
   double error = 1.0;
   int status = HR_OK;
   bool need_true_check = o.true_residual != 0 || o.precision != HR_FP64;
-  int fp64_tail = 0;  // after a failed true-residual check, stay in FP64
+  int fp64_tail = 0;  // after a refinement cycle that stalled, stay in FP64
   for (;;) {
     double r_norm = dev_norm(P, r);
     error = r_norm / bscale;
@@ -584,20 +588,22 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
       status = HR_ERR_NAN;
       break;
     }
+    if (refine && R.restarts > 0) R.true_residual = error;
     if (error <= o.tol || iter >= max_iter) break;
+    const double err_start = error;
+    const double cycle_tol = (refine && !fp64_tail) ? std::max(0.5 * o.tol, eta * err_start) : o.tol;
     launch_copy(n, r, P.V.p, st);
     launch_scale_host(n, 1.0 / r_norm, P.V.p, st);
     C.launches += 2;
     std::fill(g.begin(), g.end(), 0.0);
     g[0] = r_norm;
     int j = -1;
-    double err_prev = error;
-    while (j < m - 1 && error > o.tol && iter < max_iter) {
+    while (j < m - 1 && error > cycle_tol && iter < max_iter) {
       j++;
       iter++;
       double* vj = P.V.p + (size_t)j * n;
       double* w = P.V.p + (size_t)(j + 1) * n;
-      int prec = (relax > 0 && !fp64_tail && err_prev <= relax) ? o.precision : HR_FP64;
+      const int prec = (refine && !fp64_tail) ? o.precision : HR_FP64;
       plan_matvec(P, vj, w, prec);
       if (prec) R.matvecs_mixed++;
       else R.matvecs_fp64++;
@@ -633,7 +639,6 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
       Hm(j + 1, j) = 0.0;
       g[j + 1] = -sn[j] * g[j];
       g[j] = cs[j] * g[j];
-      err_prev = error;
       error = fabs(g[j + 1]) / bscale;
       if (iter - 1 < 512) R.resid_hist[iter - 1] = error;
       if (!std::isfinite(error)) {
@@ -661,11 +666,15 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
     R.matvecs_fp64++;
     launch_sub(n, b_dev, r, r, st);
     C.launches++;
+    if (refine) {
+      const double tr = dev_norm(P, r) / bscale;
+      if (!(tr <= 0.5 * err_start)) fp64_tail = 1;  // the reduced-precision cycle stalled
+      continue;  // the loop head tests the FP64 residual
+    }
     if (converged) {
       double tr = dev_norm(P, r) / bscale;
       R.true_residual = tr;
       if (tr <= o.tol * 10.0 || iter >= max_iter) break;
-      fp64_tail = 1;  // the relaxed iterates drifted: finish in FP64
     }
   }
   if (status == HR_OK && need_true_check && R.true_residual < 0) {
@@ -681,6 +690,7 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  C.check_tc();
   R.iterations = iter;
   R.residual = error;
   R.seconds = ms * 1e-3;
@@ -768,6 +778,7 @@ extern "C" int hr_plan2s_matvec_dev(hr_plan2s* plan, const double* x_dev, double
     HR_REQUIRE(x_dev && y_dev, "null vector");
     HR_REQUIRE(precision == HR_FP64 || precision == HR_MIXED || precision == HR_FP32, "unknown precision");
     plan_matvec(*plan, x_dev, y_dev, precision);
+    if (precision != HR_FP64) plan->C->check_tc();
   });
 }
 
@@ -912,6 +923,43 @@ extern "C" int hr_measure_fp64_peak(hr_ctx* ctx, double* flops_per_s) {
     ctx->c.launches += 2;
     double fl = 2.0 * 8.0 * (double)iters * blocks * 256;
     *flops_per_s = fl / (ms * 1e-3);
+  });
+}
+
+extern "C" int hr_plan2s_check_upward_pass(hr_plan2s* plan, const double* x, double* max_rel_err) {
+  if (!plan || !x || !max_rel_err) return HR_ERR_ARG;
+  return guard(ctx_of(plan), [&] {
+    hr_plan2s& P = *plan;
+    Ctx& C = *P.C;
+    cudaStream_t st = C.stream;
+    HR_REQUIRE(P.opt.mode == HR_TREE, "the upward pass exists in tree mode only");
+    HR_CHECK_CUDA(cudaMemcpyAsync(P.xin.p, x, sizeof(double) * P.n, cudaMemcpyHostToDevice, st));
+    double worst = 0.0;
+    for (int s = 0; s < 2; s++) {
+      DevTree& T = P.tree[s];
+      const size_t m = (size_t)T.nn * 12 * T.Pf;
+      std::vector<double> a(m), b(m);
+      T.set_density(C, P.xin.p + P.off[s], true, true, false);
+      HR_CHECK_CUDA(cudaMemcpyAsync(a.data(), T.mom.p, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+      HR_CHECK_CUDA(cudaStreamSynchronize(st));
+      T.set_density(C, P.xin.p + P.off[s], true, true, true);
+      HR_CHECK_CUDA(cudaMemcpyAsync(b.data(), T.mom.p, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+      HR_CHECK_CUDA(cudaStreamSynchronize(st));
+      C.check_tc();
+      // per node and channel, relative to that channel's largest FP64 moment
+      for (int nd = 0; nd < T.nn; nd++)
+        for (int c = 0; c < 12; c++) {
+          const double* pa = a.data() + ((size_t)nd * 12 + c) * T.Pf;
+          const double* pb = b.data() + ((size_t)nd * 12 + c) * T.Pf;
+          double mx = 0.0, dif = 0.0;
+          for (int k = 0; k < T.Pf; k++) {
+            mx = std::max(mx, fabs(pa[k]));
+            dif = std::max(dif, fabs(pa[k] - pb[k]));
+          }
+          if (mx > 0.0) worst = std::max(worst, dif / mx);
+        }
+    }
+    *max_rel_err = worst;
   });
 }
 

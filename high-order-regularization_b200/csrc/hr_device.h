@@ -75,6 +75,22 @@ struct MomItem {
   int s1;  // one past last source
   int out; // partial slot
 };
+// Poisson extension (solve_Poisson, E2G/main.cpp:969-1044) with a reusable
+// work area (FFT plan, tables, grid buffers) for one grid size N.
+struct PoissonWork;
+PoissonWork* poisson_work_create(struct Ctx& C, int N);
+void poisson_work_destroy(PoissonWork* w);
+void solve_poisson_dev(struct Ctx& C, int N, double L, const uint8_t* band2_dev, const uint8_t* out_dev,
+                       const double* p_dev, double* u_dev, int variable, PoissonWork* work = nullptr);
+
+// Tensor-core (tcgen05, 3xTF32) upward pass for the reduced-precision operator:
+// same items and partial layout as launch_moments; a timed-out wait sets *err.
+bool moments_tc_supported(int P1);
+size_t moments_tc_smem(int dl, int P1, int* npad, int* cols);
+void launch_moments_tc(int dl, const MomItem* d_items, int nitems, int P1, const double* tcheb, const double* x,
+                       const double* y, const double* z, const double* nx, const double* ny, const double* nz,
+                       const double* a, const double* qx, const double* qy, const double* qz, double* partial,
+                       int* err, cudaStream_t st);
 void launch_moments(int dl, const MomItem* d_items, int nitems, int P1, const double* tcheb,
                     const double* x, const double* y, const double* z, const double* nx,
                     const double* ny, const double* nz, const double* a, const double* qx,

@@ -15,11 +15,6 @@
 #include "../host/hr_e2g_geom.h"
 #include "hr_runtime.h"
 
-namespace hr {
-void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const uint8_t* out_dev,
-                       const double* p_dev, double* u_dev, int variable);
-}
-
 using namespace hr;
 
 namespace {
@@ -208,6 +203,8 @@ struct hr_e2g {
   bool have_ref = false;
   Batch batch[3];                         // by precision: FP64, mixed, all FP32
   long long pairs = 0;
+  PoissonWork* pw = nullptr;              // FFT plan and grid buffers of the four Poisson solves
+  ~hr_e2g() { poisson_work_destroy(pw); }
 };
 
 extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
@@ -397,10 +394,11 @@ extern "C" int hr_e2g_run(hr_e2g* E, int precision, hr_e2g_report* rep) {
     HR_CHECK_CUDA(cudaEventRecord(ev[2], st));
     // Poisson extensions: p (variable 0) then u_x, u_y, u_z with the extended p
     HR_CHECK_CUDA(cudaMemcpyAsync(E->p_ext.p, E->p_bi.p, sizeof(double) * m3, cudaMemcpyDeviceToDevice, st));
-    solve_poisson_dev(C, N, E->S.L, E->mband2.p, E->mout.p, nullptr, E->p_ext.p, 0);
+    if (!E->pw) E->pw = poisson_work_create(C, N);
+    solve_poisson_dev(C, N, E->S.L, E->mband2.p, E->mout.p, nullptr, E->p_ext.p, 0, E->pw);
     HR_CHECK_CUDA(cudaMemcpyAsync(E->u_ext.p, E->u_bi.p, sizeof(double) * 3 * m3, cudaMemcpyDeviceToDevice, st));
     for (int v = 0; v < 3; v++)
-      solve_poisson_dev(C, N, E->S.L, E->mband2.p, E->mout.p, E->p_ext.p, E->u_ext.p + v * m3, v + 1);
+      solve_poisson_dev(C, N, E->S.L, E->mband2.p, E->mout.p, E->p_ext.p, E->u_ext.p + v * m3, v + 1, E->pw);
     HR_CHECK_CUDA(cudaEventRecord(ev[3], st));
     HR_CHECK_CUDA(cudaEventSynchronize(ev[3]));
     float t01 = 0, t23 = 0, t03 = 0;

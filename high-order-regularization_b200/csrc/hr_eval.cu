@@ -12,13 +12,18 @@
 //                    in shared memory (Call_Treecode_*, 2S/KITC.cpp:671-777).
 // A warp whose mask word is zero for an entry skips the arithmetic entirely.
 //
-// Precision. FP64: every pair in FP64. MIXED: every pair with r > 3 delta is
-// evaluated in FP32 from centre-relative FP32 coordinates (the plain kernels
-// of far targets, the regularized kernels with erff/expf for 3 delta < r <=
-// 8 delta, the subtraction forms of near targets, and all proxy
-// interactions), summed per 16 terms in FP32 and added to the FP64
-// per-target accumulators; the r <= 3 delta pairs, where the smoothing
-// brackets cancel, stay in FP64.
+// Precision. FP64: every pair in FP64. MIXED: FP32 pairs from FP32
+// coordinates relative to the target block's first target, summed per 16
+// terms in FP32 and added to the FP64 per-target accumulators:
+//   * on-surface kinds: every pair, the smoothing factors from FP32
+//     piecewise polynomials in s = r^2/delta^2 (no erf / exp, and no
+//     cancellation at any r);
+//   * off-surface kinds: pairs with r > 3 delta (the plain kernels of far
+//     targets, the regularized kernels with erff / expf, the subtraction
+//     forms) in FP32; pairs with r <= 3 delta, where the erf / exp brackets
+//     with the target's coefficients cancel, in FP64;
+//   * all proxy interactions in FP32.
+// FP32 (all pairs): as MIXED with every off-surface pair in FP32 too.
 #include <cstdio>
 
 #include "hr_device.h"
@@ -39,6 +44,21 @@ namespace {
 // relative error; G(0) is the reference's r -> 0 value. The table of a kernel
 // family is staged in shared memory once per CTA.
 constexpr int kSmoothN = HR_SMOOTH_PIECES * (HR_SMOOTH_DEG + 2);
+
+constexpr int kSmooth32N = HR_SMOOTH32_PIECES * 8;  // floats per FP32 table
+
+// FP32 piece: (centre, c0, c1, c2) (c3, c4, c5, 0); index floor(s * pieces / 64)
+// for 0 <= s <= 64, formed on the FMA / ALU pipes: adding 1.5 * 2^23 to
+// s * pieces / 64 - 1/2 leaves round-to-nearest of it, i.e. the floor (a tie
+// picks the lower piece, whose polynomial covers its right end), in the low
+// mantissa bits.
+__device__ __forceinline__ float smooth_eval_f(const float4* __restrict__ tab, float s) {
+  const float f = fmaf(s, HR_SMOOTH32_PIECES / 64.0f, -0.5f) + 12582912.0f;
+  const int i = min(__float_as_int(f) - 0x4B400000, HR_SMOOTH32_PIECES - 1);
+  const float4 a = tab[2 * i], b = tab[2 * i + 1];
+  const float t = s - a.x;
+  return fmaf(fmaf(fmaf(fmaf(fmaf(b.z, t, b.y), t, b.x), t, a.w), t, a.z), t, a.y);
+}
 
 __device__ __forceinline__ double smooth_eval(const double* __restrict__ tab, double s) {
   int i = (int)(sqrtf((float)s) * (HR_SMOOTH_PIECES / 8.0f));
@@ -66,18 +86,18 @@ struct Tgt {
 };
 
 struct Tgt32 {
-  float px, py, pz;  // relative to the source surface centre
+  float px, py, pz;  // relative to the FP32 origin of the target block
   float f0n0;        // 0 for targets without subtraction
   float g0[3];
   float n0xf0[3];
   float b;
-  float x0[3];       // relative to the source surface centre
+  float x0[3];       // relative to the FP32 origin of the target block
   float n0[3];
   CoefF c;
 };
 
 template <int KIND>
-__device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid, Tgt& S,
+__device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid, const double* cb, Tgt& S,
                                             Tgt32& F) {
   S.px = S.py = S.pz = 0.0;
   S.b = 0.0;
@@ -127,9 +147,9 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
       S.c = reg_coeff(S.b / T.DEL);
     }
   }
-  F.px = (float)(S.px - T.ctr[0]);
-  F.py = (float)(S.py - T.ctr[1]);
-  F.pz = (float)(S.pz - T.ctr[2]);
+  F.px = (float)(S.px - cb[0]);
+  F.py = (float)(S.py - cb[1]);
+  F.pz = (float)(S.pz - cb[2]);
   // the direct sum of a far Stokeslet target has no subtraction (2S/KITC.cpp:856-882),
   // nor has the plain stresslet of a far target (2S/KITC.cpp:970-995)
   F.f0n0 = (KIND == K_SL_OFF && !S.near) ? 0.0f : (float)S.f0n0;
@@ -137,7 +157,7 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
   for (int k = 0; k < 3; k++) {
     F.g0[k] = no_g0 ? 0.0f : (float)S.g0[k];
     F.n0xf0[k] = (float)S.n0xf0[k];
-    F.x0[k] = (float)(S.x0[k] - T.ctr[k]);
+    F.x0[k] = (float)(S.x0[k] - cb[k]);
     F.n0[k] = (float)S.n0[k];
   }
   F.b = (float)S.b;
@@ -306,56 +326,50 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
 // The singular kernel of each kind (the r/delta > 8 branch of the reference),
 // from FP32 centre-relative coordinates.
 template <int KIND>
-__device__ __forceinline__ void pair32(const float* __restrict__ sf, int j, const Tgt32& F,
+__device__ __forceinline__ void pair32(const float4* __restrict__ s4, int j, const Tgt32& F,
                                        float& p0, float& p1, float& p2) {
-  const float* X = sf;
-  const float* Y = sf + kNT;
-  const float* Z = sf + 2 * kNT;
-  const float* NX = sf + 3 * kNT;
-  const float* NY = sf + 4 * kNT;
-  const float* NZ = sf + 5 * kNT;
-  const float* A = sf + 6 * kNT;
-  const float* QX = sf + 7 * kNT;
-  const float* QY = sf + 8 * kNT;
-  const float* QZ = sf + 9 * kNT;
-  const float dx = F.px - X[j], dy = F.py - Y[j], dz = F.pz - Z[j];
+  constexpr bool kNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY);
+  const float4 P = s4[j];  // x, y, z, area
+  const float4 N = kNrm ? s4[kNT + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 Q = s4[2 * kNT + j];
+  const float dx = F.px - P.x, dy = F.py - P.y, dz = F.pz - P.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = rsqrtf(r2);
   const float rinv2 = rinv * rinv;
   if (KIND == K_E2G_SL_AWAY) {
     // plain Stokeslet, no subtraction; the face sums stage no normals
-    const float fx = QX[j], fy = QY[j], fz = QZ[j];
+    const float fx = Q.x, fy = Q.y, fz = Q.z;
     const float fdd = fx * dx + fy * dy + fz * dz;
-    const float H1 = A[j] * rinv;
+    const float H1 = P.w * rinv;
     const float H2 = fdd * H1 * rinv2;
     p0 += fx * H1 + dx * H2;
     p1 += fy * H1 + dy * H2;
     p2 += fz * H1 + dz * H2;
   } else if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7) {
-    const float fx = QX[j] - F.f0n0 * NX[j];
-    const float fy = QY[j] - F.f0n0 * NY[j];
-    const float fz = QZ[j] - F.f0n0 * NZ[j];
+    const float fx = Q.x - F.f0n0 * N.x;
+    const float fy = Q.y - F.f0n0 * N.y;
+    const float fz = Q.z - F.f0n0 * N.z;
     const float fdd = fx * dx + fy * dy + fz * dz;
-    const float H1 = A[j] * rinv;
+    const float H1 = P.w * rinv;
     const float H2 = fdd * H1 * rinv2;
     p0 += fx * H1 + dx * H2;
     p1 += fy * H1 + dy * H2;
     p2 += fz * H1 + dz * H2;
   } else if (KIND == K_DL_ON || KIND == K_DL_OFF) {
-    const float gx = QX[j] - F.g0[0];
-    const float gy = QY[j] - F.g0[1];
-    const float gz = QZ[j] - F.g0[2];
+    const float gx = Q.x - F.g0[0];
+    const float gy = Q.y - F.g0[1];
+    const float gz = Q.z - F.g0[2];
     const float gdd = gx * dx + gy * dy + gz * dz;
-    const float ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
-    const float kernel = ndd * gdd * (rinv2 * rinv2 * rinv) * A[j];
+    const float ndd = N.x * dx + N.y * dy + N.z * dz;
+    const float kernel = ndd * gdd * (rinv2 * rinv2 * rinv) * P.w;
     p0 += dx * kernel;
     p1 += dy * kernel;
     p2 += dz * kernel;
   } else if (KIND == K_E2G_P_AWAY) {
-    p0 += (QX[j] * dx + QY[j] * dy + QZ[j] * dz) * (rinv2 * rinv) * A[j];
+    p0 += (Q.x * dx + Q.y * dy + Q.z * dz) * (rinv2 * rinv) * P.w;
   } else if (KIND == K_E2G_P7) {
-    const float n0 = NX[j], n1 = NY[j], n2 = NZ[j];
-    const float f0 = QX[j], f1 = QY[j], f2 = QZ[j];
+    const float n0 = N.x, n1 = N.y, n2 = N.z;
+    const float f0 = Q.x, f1 = Q.y, f2 = Q.z;
     const float f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
     const float ncf0 = (n1 * f2 - n2 * f1) - F.n0xf0[0];
     const float ncf1 = (n2 * f0 - n0 * f2) - F.n0xf0[1];
@@ -366,7 +380,58 @@ __device__ __forceinline__ void pair32(const float* __restrict__ sf, int j, cons
     const float ncd2 = n0 * dy - n1 * dx;
     const float normal = -(f_dot_n - F.f0n0) * n_dot_dx;
     const float tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
-    p0 += (normal + tangential) * (rinv2 * rinv) * A[j];
+    p0 += (normal + tangential) * (rinv2 * rinv) * P.w;
+  }
+}
+
+// ------------------------------------- FP32 on-surface pairs, all distances
+// Call_Ds_SL_onSurf / Call_Ds_DL_onSurf (2S/KITC.cpp:807-846, 921-957) in
+// FP32: the smoothing factor from the FP32 table for s = r^2/delta^2 <= 64,
+// the singular kernel beyond (a branch that only warps at the 8 delta
+// boundary split on).
+template <int KIND>
+__device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, const Tgt32& F, const RegF& gf,
+                                          const float4* __restrict__ tab, float& p0, float& p1, float& p2) {
+  const float4 P = s4[j];  // x, y, z, area
+  const float4 N = s4[kNT + j];
+  const float4 Q = s4[2 * kNT + j];
+  const float dx = F.px - P.x, dy = F.py - P.y, dz = F.pz - P.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float sq = r2 * gf.inv_d2;
+  if (KIND == K_SL_ON) {
+    const float fx = Q.x - F.f0n0 * N.x;
+    const float fy = Q.y - F.f0n0 * N.y;
+    const float fz = Q.z - F.f0n0 * N.z;
+    const float fdd = fx * dx + fy * dy + fz * dz;
+    float H1, H2;
+    if (sq <= 64.0f) {
+      H1 = smooth_eval_f(tab, sq) * gf.inv_d;
+      H2 = smooth_eval_f(tab + kSmooth32N / 4, sq) * gf.inv_d3;
+    } else {
+      H1 = rsqrtf(r2);
+      H2 = H1 * H1 * H1;
+    }
+    const float h1 = H1 * P.w, h2 = H2 * P.w * fdd;
+    p0 += fx * h1 + dx * h2;
+    p1 += fy * h1 + dy * h2;
+    p2 += fz * h1 + dz * h2;
+  } else {  // K_DL_ON
+    const float gx = Q.x - F.g0[0];
+    const float gy = Q.y - F.g0[1];
+    const float gz = Q.z - F.g0[2];
+    const float gdd = gx * dx + gy * dy + gz * dz;
+    const float ndd = N.x * dx + N.y * dy + N.z * dz;
+    float H3;
+    if (sq <= 64.0f) {
+      H3 = smooth_eval_f(tab, sq) * gf.inv_d5;
+    } else {
+      const float ri = rsqrtf(r2), ri2 = ri * ri;
+      H3 = ri2 * ri2 * ri;
+    }
+    const float kernel = ndd * gdd * H3 * P.w;
+    p0 += dx * kernel;
+    p1 += dy * kernel;
+    p2 += dz * kernel;
   }
 }
 
@@ -376,65 +441,58 @@ __device__ __forceinline__ void pair32(const float* __restrict__ sf, int j, cons
 // subtraction), in FP32 for pairs with r > 3 delta. Returns true if the
 // smoothed branch was taken.
 template <int KIND>
-__device__ __forceinline__ bool pair32r(const float* __restrict__ sf, int j, const Tgt32& F, const RegF& gf,
+__device__ __forceinline__ bool pair32r(const float4* __restrict__ s4, int j, const Tgt32& F, const RegF& gf,
                                         float& p0, float& p1, float& p2) {
-  const float* X = sf;
-  const float* Y = sf + kNT;
-  const float* Z = sf + 2 * kNT;
-  const float* NX = sf + 3 * kNT;
-  const float* NY = sf + 4 * kNT;
-  const float* NZ = sf + 5 * kNT;
-  const float* A = sf + 6 * kNT;
-  const float* QX = sf + 7 * kNT;
-  const float* QY = sf + 8 * kNT;
-  const float* QZ = sf + 9 * kNT;
-  const float dx = F.px - X[j], dy = F.py - Y[j], dz = F.pz - Z[j];
+  const float4 P = s4[j];  // x, y, z, area
+  const float4 N = s4[kNT + j];
+  const float4 Q = s4[2 * kNT + j];
+  const float dx = F.px - P.x, dy = F.py - P.y, dz = F.pz - P.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float rinv = rsqrtf(r2);
   const bool reg = r2 <= gf.d64;
   if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_E2G_SL7) {
-    const float fx = QX[j] - F.f0n0 * NX[j];
-    const float fy = QY[j] - F.f0n0 * NY[j];
-    const float fz = QZ[j] - F.f0n0 * NZ[j];
+    const float fx = Q.x - F.f0n0 * N.x;
+    const float fy = Q.y - F.f0n0 * N.y;
+    const float fz = Q.z - F.f0n0 * N.z;
     const float fdd = fx * dx + fy * dy + fz * dz;
     float H1, H2;
     if (KIND == K_SL_ON) sl_7ord_onsurf_f(r2, rinv, gf, H1, H2);
     else sl_7ord_f(r2, rinv, gf, F.c, H1, H2);
-    H1 *= A[j];
-    H2 *= A[j] * fdd;
+    H1 *= P.w;
+    H2 *= P.w * fdd;
     p0 += fx * H1 + dx * H2;
     p1 += fy * H1 + dy * H2;
     p2 += fz * H1 + dz * H2;
   } else if (KIND == K_DL_ON) {
-    const float gx = QX[j] - F.g0[0];
-    const float gy = QY[j] - F.g0[1];
-    const float gz = QZ[j] - F.g0[2];
+    const float gx = Q.x - F.g0[0];
+    const float gy = Q.y - F.g0[1];
+    const float gz = Q.z - F.g0[2];
     const float gdd = gx * dx + gy * dy + gz * dz;
-    const float ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+    const float ndd = N.x * dx + N.y * dy + N.z * dz;
     float H3;
     dl_7ord_onsurf_f(r2, rinv, gf, H3);
-    const float kernel = ndd * gdd * H3 * A[j];
+    const float kernel = ndd * gdd * H3 * P.w;
     p0 += dx * kernel;
     p1 += dy * kernel;
     p2 += dz * kernel;
   } else if (KIND == K_DL_OFF) {
     // the subtraction form of a near target (2S/KITC.cpp:996-1059)
     const float b = F.b;
-    const float xh0 = X[j] - F.x0[0], xh1 = Y[j] - F.x0[1], xh2 = Z[j] - F.x0[2];
-    const float gx = QX[j] - F.g0[0], gy = QY[j] - F.g0[1], gz = QZ[j] - F.g0[2];
+    const float xh0 = P.x - F.x0[0], xh1 = P.y - F.x0[1], xh2 = P.z - F.x0[2];
+    const float gx = Q.x - F.g0[0], gy = Q.y - F.g0[1], gz = Q.z - F.g0[2];
     const float sig_sq = (xh0 * xh0 + xh1 * xh1 + xh2 * xh2) - 2.0f * b * (xh0 * F.n0[0] + xh1 * F.n0[1] + xh2 * F.n0[2]);
     const float g_dot_n0 = gx * F.n0[0] + gy * F.n0[1] + gz * F.n0[2];
     const float g_dot_xh = gx * xh0 + gy * xh1 + gz * xh2;
-    const float n0_dot_n = F.n0[0] * NX[j] + F.n0[1] * NY[j] + F.n0[2] * NZ[j];
-    const float xh_dot_n = xh0 * NX[j] + xh1 * NY[j] + xh2 * NZ[j];
+    const float n0_dot_n = F.n0[0] * N.x + F.n0[1] * N.y + F.n0[2] * N.z;
+    const float xh_dot_n = xh0 * N.x + xh1 * N.y + xh2 * N.z;
     const float c_m1a = g_dot_n0 * n0_dot_n;
     const float c_m1b = g_dot_xh * n0_dot_n + g_dot_n0 * xh_dot_n;
     const float c_m2a = g_dot_xh * xh_dot_n;
     const float c_m2b = b * c_m1b;
     float H2, H3;
     dl_7ord_f(r2, rinv, gf, F.c, H2, H3);
-    H2 *= A[j];
-    H3 *= A[j];
+    H2 *= P.w;
+    H3 *= P.w;
     float m1 = dx * c_m1a - F.n0[0] * c_m1b;
     float m2 = -sig_sq * m1 + dx * c_m2a + xh0 * c_m2b;
     p0 += m1 * H2 + m2 * H3;
@@ -447,8 +505,8 @@ __device__ __forceinline__ bool pair32r(const float* __restrict__ sf, int j, con
   } else if (KIND == K_E2G_P7) {
     float H2;
     lapl_dl_7ord_f(r2, rinv, gf, F.c, H2);
-    const float n0 = NX[j], n1 = NY[j], n2 = NZ[j];
-    const float f0 = QX[j], f1 = QY[j], f2 = QZ[j];
+    const float n0 = N.x, n1 = N.y, n2 = N.z;
+    const float f0 = Q.x, f1 = Q.y, f2 = Q.z;
     const float f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
     const float ncf0 = (n1 * f2 - n2 * f1) - F.n0xf0[0];
     const float ncf1 = (n2 * f0 - n0 * f2) - F.n0xf0[1];
@@ -459,7 +517,7 @@ __device__ __forceinline__ bool pair32r(const float* __restrict__ sf, int j, con
     const float ncd2 = n0 * dy - n1 * dx;
     const float normal = -(f_dot_n - F.f0n0) * n_dot_dx;
     const float tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
-    p0 += (normal + tangential) * H2 * A[j];
+    p0 += (normal + tangential) * H2 * P.w;
   }
   return reg;
 }
@@ -562,20 +620,37 @@ __device__ __forceinline__ void proxies32(const float* __restrict__ sf, int PT, 
 
 template <int KIND, bool MIXED>
 __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
-                                         const Seg* __restrict__ segs, double* sm, float* sf,
-                                         double* cheb, float* chebf, const double* stab) {
+                                         const Seg* __restrict__ segs, double* sm, float4* s4,
+                                         double* cheb, float* chebf, const double* stab,
+                                         const float4* stab32) {
+  float* sf = reinterpret_cast<float*>(s4);  // proxy moments (FP32) share the tile buffer
+  constexpr bool kCount = !MIXED;            // work counters come from the FP64 launches
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int blk = it.blk;
   const int k = blk * kTB + tid;
   const bool valid = k < T.nt;
   const int t = valid ? T.tord[k] : 0;
+  // origin of the FP32 coordinates: the block's first target (the sources a
+  // block meets lie within a few leaf sizes of it, so FP32 offsets stay small)
+  double cb[3];
+  {
+    const int t0 = T.tord[blk * kTB];
+    cb[0] = T.txyz[3 * t0];
+    cb[1] = T.txyz[3 * t0 + 1];
+    cb[2] = T.txyz[3 * t0 + 2];
+  }
   Tgt S;
   Tgt32 F;
-  load_target<KIND>(T, t, valid, S, F);
+  load_target<KIND>(T, t, valid, cb, S, F);
   const Reg g = make_reg(T.DEL);
   RegF gf;
   gf.inv_d = (float)g.inv_d;
   gf.d64 = (float)g.d64;
+  gf.inv_d2 = (float)g.inv_d2;
+  gf.inv_d3 = (float)g.inv_d3;
+  gf.inv_d5 = (float)g.inv_d5;
+  // on-surface kinds in the reduced-precision modes: every pair in FP32
+  constexpr bool kOn32 = MIXED && (KIND == K_SL_ON || KIND == K_DL_ON);
   // FP64 below, FP32 above: (3 delta)^2 in the mixed mode; in the all-FP32 mode
   // only the r < 1e-14 limits of the reference stay in FP64
   const float cut2f = T.mixed == 2 ? 1e-28f : (float)(9.0 * T.DEL * T.DEL);
@@ -599,71 +674,73 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
         __syncthreads();
         for (int i = tid; i < cnt; i += kTB) {
           const int s = s0 + i;
-          sm[i] = T.sx[s];
-          sm[kNT + i] = T.sy[s];
-          sm[2 * kNT + i] = T.sz[s];
-          if (kSrcNrm) {
-            sm[3 * kNT + i] = T.snx[s];
-            sm[4 * kNT + i] = T.sny[s];
-            sm[5 * kNT + i] = T.snz[s];
-          }
-          sm[6 * kNT + i] = T.sa[s];
-          sm[7 * kNT + i] = T.qx[s];
-          sm[8 * kNT + i] = T.qy[s];
-          sm[9 * kNT + i] = T.qz[s];
-          if (MIXED) {
-            sf[i] = T.fx[s];
-            sf[kNT + i] = T.fy[s];
-            sf[2 * kNT + i] = T.fz[s];
+          const double x = T.sx[s], y = T.sy[s], z = T.sz[s];
+          if (!kOn32) {
+            sm[i] = x;
+            sm[kNT + i] = y;
+            sm[2 * kNT + i] = z;
             if (kSrcNrm) {
-              sf[3 * kNT + i] = T.fnx[s];
-              sf[4 * kNT + i] = T.fny[s];
-              sf[5 * kNT + i] = T.fnz[s];
+              sm[3 * kNT + i] = T.snx[s];
+              sm[4 * kNT + i] = T.sny[s];
+              sm[5 * kNT + i] = T.snz[s];
             }
-            sf[6 * kNT + i] = T.fa[s];
-            sf[7 * kNT + i] = T.fqx[s];
-            sf[8 * kNT + i] = T.fqy[s];
-            sf[9 * kNT + i] = T.fqz[s];
+            sm[6 * kNT + i] = T.sa[s];
+            sm[7 * kNT + i] = T.qx[s];
+            sm[8 * kNT + i] = T.qy[s];
+            sm[9 * kNT + i] = T.qz[s];
+          }
+          if (MIXED) {
+            s4[i] = make_float4((float)(x - cb[0]), (float)(y - cb[1]), (float)(z - cb[2]), T.fa[s]);
+            if (kSrcNrm) s4[kNT + i] = make_float4(T.fnx[s], T.fny[s], T.fnz[s], 0.f);
+            s4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
           }
         }
         __syncthreads();
         if (wm != 0u && act) {
-          if (all32) {
+          if (kOn32) {
             for (int j0 = 0; j0 < cnt; j0 += 16) {
               float p0 = 0.f, p1 = 0.f, p2 = 0.f;
               const int j1 = min(cnt, j0 + 16);
-              for (int j = j0; j < j1; j++) pair32<KIND>(sf, j, F, p0, p1, p2);
+#pragma unroll 4
+              for (int j = j0; j < j1; j++) pair32tab<KIND>(s4, j, F, gf, stab32, p0, p1, p2);
               a0 += (double)p0;
               a1 += (double)p1;
               a2 += (double)p2;
             }
-            if (S.near) cplain += cnt;
-            else cfar += cnt;
+          } else if (all32) {
+            for (int j0 = 0; j0 < cnt; j0 += 16) {
+              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+              const int j1 = min(cnt, j0 + 16);
+              for (int j = j0; j < j1; j++) pair32<KIND>(s4, j, F, p0, p1, p2);
+              a0 += (double)p0;
+              a1 += (double)p1;
+              a2 += (double)p2;
+            }
           } else if (MIXED && kPerPairSplit && S.near) {
-            unsigned cr = 0;
             for (int j0 = 0; j0 < cnt; j0 += 16) {
               float p0 = 0.f, p1 = 0.f, p2 = 0.f;
               const int j1 = min(cnt, j0 + 16);
               for (int j = j0; j < j1; j++) {
-                const float dx = F.px - sf[j], dy = F.py - sf[kNT + j], dz = F.pz - sf[2 * kNT + j];
-                if (dx * dx + dy * dy + dz * dz > cut2f) cr += pair32r<KIND>(sf, j, F, gf, p0, p1, p2);
-                else cr += pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
+                const float4 Pj = s4[j];
+                const float dx = F.px - Pj.x, dy = F.py - Pj.y, dz = F.pz - Pj.z;
+                if (dx * dx + dy * dy + dz * dz > cut2f) pair32r<KIND>(s4, j, F, gf, p0, p1, p2);
+                else pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
               }
               a0 += (double)p0;
               a1 += (double)p1;
               a2 += (double)p2;
             }
-            creg += cr;
-            cplain += cnt - cr;
           } else {
             unsigned cr = 0;
 #pragma unroll 2
             for (int j = 0; j < cnt; j++) cr += pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
-            if (S.near) {
-              creg += cr;
-              cplain += cnt - cr;
-            } else {
-              cfar += cnt;
+            if (kCount) {
+              if (S.near) {
+                creg += cr;
+                cplain += cnt - cr;
+              } else {
+                cfar += cnt;
+              }
             }
           }
         }
@@ -676,7 +753,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
       if (tid < 3 * P1) {
         const double v = T.tcheb[(size_t)E.node * 3 * P1 + tid];
         cheb[tid] = v;
-        if (MIXED) chebf[tid] = (float)(v - T.ctr[tid / P1]);
+        if (MIXED) chebf[tid] = (float)(v - cb[tid / P1]);
       }
       const double* M = T.mom + (size_t)E.node * C * Pf;
       for (int kk0 = 0; kk0 < Pf; kk0 += PT) {
@@ -701,7 +778,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           } else {
             proxies64<DL>(sm, PT, cnt, kk0, P1, cheb, S, a0, a1, a2);
           }
-          cprox += cnt;
+          if (kCount) cprox += cnt;
         }
       }
     }
@@ -712,7 +789,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   o[1] = a1;
   o[2] = a2;
   // Work counters (pair kinds actually evaluated), one atomic per warp.
-  if (T.counters) {
+  if (kCount && T.counters) {
     for (int off = 16; off > 0; off >>= 1) {
       creg += __shfl_down_sync(0xffffffffu, creg, off);
       cplain += __shfl_down_sync(0xffffffffu, cplain, off);
@@ -733,12 +810,15 @@ __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict
                                                       const BlockRef* __restrict__ items,
                                                       const Seg* __restrict__ segs) {
   __shared__ double sm[kSmem];
-  __shared__ float sf[MIXED ? kSmem : 1];
+  // FP32 source tile: (x, y, z, area), (n, 0), (q, 0) per source; also holds
+  // FP32 proxy moments (kSmem floats at most)
+  __shared__ float4 sf[MIXED ? 3 * kNT : 1];
   __shared__ double cheb[3 * kMaxP1];
   __shared__ float chebf[3 * kMaxP1];
   __shared__ EvalTask sT;
   // smoothing tables: G1, G2 for the Stokeslet family, G3 for the stresslet family
   __shared__ double stab[FAM == F_SL ? 2 * kSmoothN : (FAM == F_DL ? kSmoothN : 1)];
+  __shared__ float4 stab32[MIXED ? (FAM == F_SL ? 2 * kSmooth32N / 4 : (FAM == F_DL ? kSmooth32N / 4 : 1)) : 1];
   const BlockRef it = items[blockIdx.x];
   if (threadIdx.x == 0) sT = tasks[it.task];
   if (FAM == F_SL) {
@@ -749,20 +829,31 @@ __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict
   } else if (FAM == F_DL) {
     for (int i = threadIdx.x; i < kSmoothN; i += blockDim.x) stab[i] = kSmoothG3[i];
   }
+  if (MIXED && FAM != F_E2G) {
+    float* t32 = reinterpret_cast<float*>(stab32);
+    for (int i = threadIdx.x; i < kSmooth32N; i += blockDim.x) {
+      if (FAM == F_SL) {
+        t32[i] = kSmooth32G1[i];
+        t32[kSmooth32N + i] = kSmooth32G2[i];
+      } else {
+        t32[i] = kSmooth32G3[i];
+      }
+    }
+  }
   __syncthreads();
   const int kind = sT.kind;
   if (FAM == F_SL) {
-    if (kind == K_SL_ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
-    else run_item<K_SL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
+    if (kind == K_SL_ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    else run_item<K_SL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else if (FAM == F_DL) {
-    if (kind == K_DL_ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
-    else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab);
+    if (kind == K_DL_ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else {
     switch (kind) {
-      case K_E2G_SL_AWAY: run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
-      case K_E2G_P_AWAY: run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
-      case K_E2G_SL7: run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
-      default: run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab); break;
+      case K_E2G_SL_AWAY: run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
+      case K_E2G_P_AWAY: run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
+      case K_E2G_SL7: run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
+      default: run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
     }
   }
 }

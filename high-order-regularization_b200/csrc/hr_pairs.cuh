@@ -214,7 +214,8 @@ __device__ __forceinline__ bool lapl_dl_7ord(double r2, double rinv, const Reg& 
 namespace hr {
 
 struct RegF {
-  float inv_d, d64;  // 1/delta, 64 delta^2
+  float inv_d, d64;             // 1/delta, 64 delta^2
+  float inv_d2, inv_d3, inv_d5;  // 1/delta^k for the tabulated on-surface factors
 };
 
 struct CoefF {

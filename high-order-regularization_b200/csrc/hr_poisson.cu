@@ -17,6 +17,7 @@
 #include <cufft.h>
 
 #include <cmath>
+#include <memory>
 #include <vector>
 
 #include "hr_runtime.h"
@@ -251,15 +252,40 @@ void dst_poisson3d_dev(Ctx& C, int n, double* f_dev) {
   HR_CHECK_CUDA(cudaGetLastError());
 }
 
+// The FFT plan, twiddle tables and grid work buffers of one grid size, kept
+// across solves (a pipeline runs four solves per evaluation).
+struct PoissonWork {
+  int N = 0;
+  DstPlan P;
+  DBuf<double> w, rhs;
+};
+
+PoissonWork* poisson_work_create(Ctx& C, int N) {
+  std::unique_ptr<PoissonWork> W(new PoissonWork);
+  W->N = N;
+  const long M = N + 1;
+  const int n = N - 1;
+  W->w.alloc(M * M * M);
+  W->rhs.alloc((size_t)n * n * n);
+  W->P.make(C, n);
+  return W.release();
+}
+
+void poisson_work_destroy(PoissonWork* W) { delete W; }
+
 void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const uint8_t* out_dev,
-                       const double* p_dev, double* u_dev, int variable) {
+                       const double* p_dev, double* u_dev, int variable, PoissonWork* work) {
+  std::unique_ptr<PoissonWork> own;
+  if (!work || work->N != N) {
+    own.reset(poisson_work_create(C, N));
+    work = own.get();
+  }
   const double h = L / N;
   const long M = N + 1;
   const long m3 = M * M * M;
   const int n = N - 1;
-  DBuf<double> w, rhs;
-  w.alloc(m3);
-  rhs.alloc((size_t)n * n * n);
+  DBuf<double>& w = work->w;
+  DBuf<double>& rhs = work->rhs;
   extend_kernel<<<(int)((m3 + 255) / 256), 256, 0, C.stream>>>(N, L, h, u_dev, w.p);
   const int axis = (variable >= 1 && variable <= 3) ? variable - 1 : -1;
   long n3 = (long)n * n * n;
@@ -267,14 +293,14 @@ void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const 
                                                             p_dev, axis, rhs.p);
   C.launches += 2;
   HR_CHECK_CUDA(cudaGetLastError());
-  DstPlan P;
-  P.make(C, n);
+  DstPlan& P = work->P;
   P.dst3(C, rhs.p, 1, 0.0, nullptr, nullptr);
   // u = w everywhere, then the interior gets w + scaled solution
   HR_CHECK_CUDA(cudaMemcpyAsync(u_dev, w.p, sizeof(double) * m3, cudaMemcpyDeviceToDevice, C.stream));
   double scale = 1. / pow(2 * (n + 1), 3);
   P.dst3(C, rhs.p, 2, scale, w.p, u_dev);
-  HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
+  // a temporary work area is freed at return; its buffers must be idle first
+  if (own) HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
 }
 
 }  // namespace hr

@@ -93,10 +93,30 @@ void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direc
   mom.zero(st);
 }
 
-void DevTree::set_density(Ctx& C, const double* q3_dev, bool dl, bool moments) {
+void Ctx::check_tc() {
+  if (!tc_err.p) return;
+  int e = 0;
+  HR_CHECK_CUDA(cudaMemcpyAsync(&e, tc_err.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  HR_CHECK_CUDA(cudaStreamSynchronize(stream));
+  if (e) {
+    tc_err.zero(stream);
+    throw Error(HR_ERR_CUDA, "a tensor-core upward pass gave up waiting for its MMAs (bounded wait ran out)");
+  }
+}
+
+void DevTree::set_density(Ctx& C, const double* q3_dev, bool dl, bool moments, bool tc) {
   launch_permute(n, perm.p, q3_dev, qx.p, qy.p, qz.p, fqx.p, fqy.p, fqz.p, C.stream);
   C.launches++;
-  if (moments && nitems > 0) {
+  if (moments && nitems > 0 && tc && moments_tc_supported(P1)) {
+    if (!C.tc_err.p) {
+      C.tc_err.alloc(1);
+      C.tc_err.zero(C.stream);
+    }
+    launch_moments_tc(dl ? 1 : 0, items.p, nitems, P1, tcheb.p, x.p, y.p, z.p, nx.p, ny.p, nz.p, a.p, qx.p, qy.p,
+                      qz.p, partial.p, C.tc_err.p, C.stream);
+    launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, C.stream);
+    C.launches += 2;
+  } else if (moments && nitems > 0) {
     launch_moments(dl ? 1 : 0, items.p, nitems, P1, tcheb.p, x.p, y.p, z.p, nx.p, ny.p, nz.p, a.p,
                    qx.p, qy.p, qz.p, partial.p, C.stream);
     launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, C.stream);

@@ -81,6 +81,9 @@ struct Ctx {
   long long launches = 0;
   int num_sms = 148;
   DBuf<unsigned long long> counters;  // [0] reg pairs [1] plain pairs [2] proxies
+  DBuf<int> tc_err;                   // set by a tensor-core kernel whose bounded wait ran out
+  // throws if a tensor-core kernel of this context reported a timed-out wait
+  void check_tc();
 };
 
 // A surface on the device: sources in tree order, its tree, density buffers
@@ -102,7 +105,8 @@ struct DevTree {
   long long moment_terms = 0;  // sum over non-root nodes of Pf * members
   void build(const hr_surface& S, int P, int N0, double theta, bool direct, cudaStream_t st);
   // density (reference order, interleaved, device) -> tree-order SoA (+ moments)
-  void set_density(Ctx& C, const double* q3_dev, bool dl, bool moments);
+  // tc: the upward pass on the tensor cores (reduced-precision operator)
+  void set_density(Ctx& C, const double* q3_dev, bool dl, bool moments, bool tc = false);
 };
 
 // Target data on the device, reference order.

@@ -467,6 +467,12 @@ class Plan2S:
     def stream(self):
         return lib().hr_plan2s_stream(self.p)
 
+    def check_upward_pass(self, x):
+        """Max relative difference of the tensor-core (3xTF32) moments from the FP64 ones."""
+        v = ctypes.c_double()
+        self.ctx._check(lib().hr_plan2s_check_upward_pass(self.p, _dp(_f64(x)), ctypes.byref(v)))
+        return v.value
+
     def time_batch(self, which=0, iters=10):
         """Milliseconds per launch of one boundary-sum batch (0 DL fp64, 1 SL, 2 DL mixed)."""
         v = ctypes.c_double()

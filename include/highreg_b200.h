@@ -202,14 +202,16 @@ typedef struct {
   int restart;         /* GMRES restart length (reference: 15, 2S/main.cpp:213) */
   int max_iter;        /* iteration cap (reference: 100) */
   double tol;          /* relative residual tolerance (reference: 1e-10) */
-  int precision;       /* HR_FP64, or HR_MIXED / HR_FP32: relaxed-precision matvecs */
+  int precision;       /* HR_FP64, or HR_MIXED / HR_FP32: reduced-precision matvecs (below) */
   int use_guess;       /* 1: x holds an initial guess on input */
   int true_residual;   /* 1: check ||b - A x|| / ||b|| with an FP64 matvec at the end */
-  /* HR_MIXED / HR_FP32: relative accuracy assumed for a reduced-precision
-   * matvec (0 = 1e-7 for HR_MIXED, whose measured max-norm relative error is
-   * 3.5e-8, and 1e-4 for HR_FP32). Relaxed GMRES (Simoncini & Szyld 2003) switches iteration k
-   * to mixed matvecs once ||r_k|| / ||b|| <= tol / mixed_accuracy; a final
-   * FP64 true residual above 10 tol sends the solve back to FP64 matvecs. */
+  /* HR_MIXED / HR_FP32 solve by iterative refinement: every Krylov matvec
+   * in the reduced precision, each GMRES cycle run until its residual falls
+   * by 10 x mixed_accuracy (or below tol / 2), then the FP64 true residual
+   * b - A x starts the next cycle; the solve ends when that FP64 residual
+   * meets tol. mixed_accuracy: relative accuracy of a reduced-precision
+   * matvec (0 = 3e-7 for HR_MIXED, whose measured max-norm relative error
+   * is 2.7e-7, and 1e-6 for HR_FP32). */
   double mixed_accuracy;
 } hr_gmres_opts;
 
@@ -253,6 +255,11 @@ typedef struct {
   long long flops;             /* algorithmic flops by the fixed per-pair convention */
 } hr_work;
 int hr_plan2s_work(hr_plan2s* plan, int which /*0 matvec, 1 rhs*/, hr_work* w);
+/* Self-check of the reduced-precision upward pass: for density x (host, n),
+ * the proxy moments of both trees from the tensor-core 3xTF32 kernel against
+ * the FP64 ones; max over nodes and channels of max |difference| / max |FP64
+ * moment|. HR_TREE plans only. */
+int hr_plan2s_check_upward_pass(hr_plan2s* plan, const double* x, double* max_rel_err);
 /* the plan's stream (cudaStream_t) for callers that enqueue their own work */
 void* hr_plan2s_stream(hr_plan2s* plan);
 /* Times `iters` back-to-back launches of one boundary-sum batch with CUDA

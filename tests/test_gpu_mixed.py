@@ -67,9 +67,11 @@ def test_mixed_solve_reaches_fp64_residual(plan32, geo32):
 
 
 def test_fp32_operator_error(plan32):
-    """All pairs in FP32 (r < 1e-14 limits excepted): the smoothing brackets
-    cancel for close pairs, so the error is larger than the mixed mode's but
-    still bounded; it is reported, and the relaxed solve below absorbs it."""
+    """All pairs in FP32 (r < 1e-14 limits excepted): the off-surface
+    smoothing brackets cancel for close pairs, so the error is at least the
+    mixed mode's (equal when the worst entry comes from the on-surface and far
+    field terms the two modes share) and stays bounded; the refined solve
+    below absorbs it."""
     n = plan32.n
     u = torch.tensor(np.random.default_rng(2).standard_normal(n), dtype=torch.float64, device="cuda")
     y64 = torch.zeros_like(u)
@@ -82,7 +84,7 @@ def test_fp32_operator_error(plan32):
     e32 = rel_err(y32.cpu().numpy(), y64.cpu().numpy())
     em = rel_err(ym.cpu().numpy(), y64.cpu().numpy())
     print('FP32 operator max-norm relative error', e32, 'mixed', em)
-    assert em < e32 < 1e-3
+    assert em <= e32 < 1e-3
 
 
 def test_fp32_solve_reaches_fp64_residual(plan32, geo32):
@@ -92,3 +94,16 @@ def test_fp32_solve_reaches_fp64_residual(plan32, geo32):
     assert r32["matvecs_mixed"] > 0
     assert r32["true_residual"] <= 1e-9
     assert rel_err(x32, x64) < 1e-8
+
+
+@pytest.mark.parametrize("P,N0", [(6, 1000), (10, 2000), (4, 300)])
+def test_tensor_core_upward_pass_matches_fp64(ctx, geo32, P, N0):
+    """The 3xTF32 tcgen05 upward pass (reduced-precision operator) against the
+    FP64 one: split TF32 products with FP32 accumulation keep ~1e-6 relative
+    accuracy per node and channel."""
+    plan = highreg.Plan2S(ctx, geo32, mode=highreg.HR_TREE, P=P, N0=N0, theta=0.6)
+    x = np.random.default_rng(5).standard_normal(plan.n)
+    e = plan.check_upward_pass(x)
+    print("upward pass, P=%d: max relative difference %.3e" % (P, e))
+    assert 0 < e < 2e-5
+    plan.close()
