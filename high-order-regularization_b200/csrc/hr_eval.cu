@@ -524,96 +524,109 @@ __device__ __forceinline__ bool pair32r(const float4* __restrict__ s4, int j, co
 
 // ------------------------------------------------------------ proxy tiles
 
+
+
+// FP64 proxy interactions of whole Chebyshev slabs: as proxies32_slabs with
+// the moments staged per proxy as double2 (DL: 6, SL: 3 per proxy, channel
+// order as in the moment array) and FP64 arithmetic throughout.
 template <bool DL>
-__device__ __forceinline__ void proxies64(const double* __restrict__ sm, int PT, int cnt, int kk0,
-                                          int P1, const double* __restrict__ cheb, const Tgt& S,
-                                          double& a0, double& a1, double& a2) {
-  int rem = kk0 % (P1 * P1);
-  int pi = kk0 / (P1 * P1), pj = rem / P1, pk = rem % P1;
-  for (int i = 0; i < cnt; i++) {
-    const double dx0 = S.px - cheb[pi];
-    const double dx1 = S.py - cheb[P1 + pj];
-    const double dx2 = S.pz - cheb[2 * P1 + pk];
-    const double r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
-    const double rinv = rsqrt(r2);
-    const double rinv2 = rinv * rinv;
-    if (!DL) {
-      // Call_Treecode_SL (2S/KITC.cpp:700-714)
-      const double m0 = sm[i] - S.f0n0 * sm[3 * PT + i];
-      const double m1 = sm[PT + i] - S.f0n0 * sm[4 * PT + i];
-      const double m2 = sm[2 * PT + i] - S.f0n0 * sm[5 * PT + i];
-      const double temp = (m0 * dx0 + m1 * dx1 + m2 * dx2) * (rinv2 * rinv);
-      a0 += m0 * rinv + temp * dx0;
-      a1 += m1 * rinv + temp * dx1;
-      a2 += m2 * rinv + temp * dx2;
-    } else {
-      // Call_Treecode_DL (2S/KITC.cpp:753-771)
-      const double M9 = sm[9 * PT + i], M10 = sm[10 * PT + i], M11 = sm[11 * PT + i];
-      double tl[3];
-#pragma unroll
-      for (int l = 0; l < 3; l++) {
-        const double ta = sm[(3 * l) * PT + i] - S.g0[l] * M9;
-        const double tb = sm[(3 * l + 1) * PT + i] - S.g0[l] * M10;
-        const double tc = sm[(3 * l + 2) * PT + i] - S.g0[l] * M11;
-        tl[l] = ta * dx0 + tb * dx1 + tc * dx2;
-      }
-      const double kernel = (tl[0] * dx0 + tl[1] * dx1 + tl[2] * dx2) * (rinv2 * rinv2 * rinv);
-      a0 += dx0 * kernel;
-      a1 += dx1 * kernel;
-      a2 += dx2 * kernel;
-    }
-    if (++pk == P1) {
-      pk = 0;
-      if (++pj == P1) {
-        pj = 0;
-        ++pi;
+__device__ __forceinline__ void proxies64_slabs(const double2* __restrict__ s2, int nslab, int pi0, int P1,
+                                                const double* __restrict__ cheb, const Tgt& S, double& a0,
+                                                double& a1, double& a2) {
+  constexpr int W = DL ? 6 : 3;  // double2 per proxy
+  const int S2 = P1 * P1;
+  for (int sl = 0; sl < nslab; sl++) {
+    const double d0 = S.px - cheb[pi0 + sl];
+    const double2* slab = s2 + sl * S2 * W;
+    for (int pj = 0; pj < P1; pj++) {
+      const double d1 = S.py - cheb[P1 + pj];
+      const double r01 = d0 * d0 + d1 * d1;
+      const double2* row = slab + pj * P1 * W;
+      for (int pk = 0; pk < P1; pk++) {
+        const double d2 = S.pz - cheb[2 * P1 + pk];
+        const double rinv = rsqrt(fma(d2, d2, r01));
+        const double2* m = row + pk * W;
+        if (DL) {
+          const double2 m01 = m[0], m23 = m[1], m45 = m[2], m67 = m[3], m89 = m[4], m1011 = m[5];
+          const double u0 = m01.x * d0 + m01.y * d1 + m23.x * d2;
+          const double u1 = m23.y * d0 + m45.x * d1 + m45.y * d2;
+          const double u2 = m67.x * d0 + m67.y * d1 + m89.x * d2;
+          const double dmd = d0 * u0 + d1 * u1 + d2 * u2;
+          const double mnd = m89.y * d0 + m1011.x * d1 + m1011.y * d2;
+          const double g0d = S.g0[0] * d0 + S.g0[1] * d1 + S.g0[2] * d2;
+          const double ri2 = rinv * rinv;
+          const double kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
+          a0 += d0 * kernel;
+          a1 += d1 * kernel;
+          a2 += d2 * kernel;
+        } else {
+          const double2 m01 = m[0], m23 = m[1], m45 = m[2];
+          const double q0 = m01.x - S.f0n0 * m23.y;
+          const double q1 = m01.y - S.f0n0 * m45.x;
+          const double q2 = m23.x - S.f0n0 * m45.y;
+          const double temp = (q0 * d0 + q1 * d1 + q2 * d2) * (rinv * rinv * rinv);
+          a0 += q0 * rinv + temp * d0;
+          a1 += q1 * rinv + temp * d1;
+          a2 += q2 * rinv + temp * d2;
+        }
       }
     }
   }
 }
 
+// FP32 proxy interactions of whole Chebyshev slabs (fixed first index i):
+// nslab slabs starting at i = pi0, moments staged per proxy as float4
+// (DL: M00 M01 M02 M10 | M11 M12 M20 M21 | M22 Mn0 Mn1 Mn2; SL: f0 f1 f2 n0 |
+// n1 n2 - -), proxies of a slab in (j, k) order. The stresslet kernel uses
+//   sum_l (sum_k (M[3l+k] - g0_l Mn_k) d_k) d_l = d.M.d - (g0.d)(Mn.d),
+// the reference's proxy sum (Call_Treecode_DL, 2S/KITC.cpp:753-771)
+// regrouped; Call_Treecode_SL (2S/KITC.cpp:700-714) as written. Partial sums
+// of one (i, j) row go to the FP64 accumulators.
 template <bool DL>
-__device__ __forceinline__ void proxies32(const float* __restrict__ sf, int PT, int cnt, int kk0,
-                                          int P1, const float* __restrict__ chebf, const Tgt32& F,
-                                          float& p0, float& p1, float& p2) {
-  int rem = kk0 % (P1 * P1);
-  int pi = kk0 / (P1 * P1), pj = rem / P1, pk = rem % P1;
-  for (int i = 0; i < cnt; i++) {
-    const float dx0 = F.px - chebf[pi];
-    const float dx1 = F.py - chebf[P1 + pj];
-    const float dx2 = F.pz - chebf[2 * P1 + pk];
-    const float r2 = dx0 * dx0 + dx1 * dx1 + dx2 * dx2;
-    const float rinv = rsqrtf(r2);
-    const float rinv2 = rinv * rinv;
-    if (!DL) {
-      const float m0 = sf[i] - F.f0n0 * sf[3 * PT + i];
-      const float m1 = sf[PT + i] - F.f0n0 * sf[4 * PT + i];
-      const float m2 = sf[2 * PT + i] - F.f0n0 * sf[5 * PT + i];
-      const float temp = (m0 * dx0 + m1 * dx1 + m2 * dx2) * (rinv2 * rinv);
-      p0 += m0 * rinv + temp * dx0;
-      p1 += m1 * rinv + temp * dx1;
-      p2 += m2 * rinv + temp * dx2;
-    } else {
-      const float M9 = sf[9 * PT + i], M10 = sf[10 * PT + i], M11 = sf[11 * PT + i];
-      float tl[3];
-#pragma unroll
-      for (int l = 0; l < 3; l++) {
-        const float ta = sf[(3 * l) * PT + i] - F.g0[l] * M9;
-        const float tb = sf[(3 * l + 1) * PT + i] - F.g0[l] * M10;
-        const float tc = sf[(3 * l + 2) * PT + i] - F.g0[l] * M11;
-        tl[l] = ta * dx0 + tb * dx1 + tc * dx2;
+__device__ __forceinline__ void proxies32_slabs(const float4* __restrict__ s4, int nslab, int pi0, int P1,
+                                                const float* __restrict__ chebf, const Tgt32& F, double& a0,
+                                                double& a1, double& a2) {
+  constexpr int W = DL ? 3 : 2;  // float4 per proxy
+  const int S2 = P1 * P1;
+  for (int sl = 0; sl < nslab; sl++) {
+    const float d0 = F.px - chebf[pi0 + sl];
+    const float4* slab = s4 + sl * S2 * W;
+    for (int pj = 0; pj < P1; pj++) {
+      const float d1 = F.py - chebf[P1 + pj];
+      const float r01 = d0 * d0 + d1 * d1;
+      const float4* row = slab + pj * P1 * W;
+      float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+      for (int pk = 0; pk < P1; pk++) {
+        const float d2 = F.pz - chebf[2 * P1 + pk];
+        const float rinv = rsqrtf(fmaf(d2, d2, r01));
+        const float4 A = row[pk * W];
+        const float4 B = row[pk * W + 1];
+        if (DL) {
+          const float4 Cc = row[pk * W + 2];
+          const float u0 = A.x * d0 + A.y * d1 + A.z * d2;
+          const float u1 = A.w * d0 + B.x * d1 + B.y * d2;
+          const float u2 = B.z * d0 + B.w * d1 + Cc.x * d2;
+          const float dmd = d0 * u0 + d1 * u1 + d2 * u2;
+          const float mnd = Cc.y * d0 + Cc.z * d1 + Cc.w * d2;
+          const float g0d = F.g0[0] * d0 + F.g0[1] * d1 + F.g0[2] * d2;
+          const float ri2 = rinv * rinv;
+          const float kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
+          p0 += d0 * kernel;
+          p1 += d1 * kernel;
+          p2 += d2 * kernel;
+        } else {
+          const float m0 = A.x - F.f0n0 * A.w;
+          const float m1 = A.y - F.f0n0 * B.x;
+          const float m2 = A.z - F.f0n0 * B.y;
+          const float temp = (m0 * d0 + m1 * d1 + m2 * d2) * (rinv * rinv * rinv);
+          p0 += m0 * rinv + temp * d0;
+          p1 += m1 * rinv + temp * d1;
+          p2 += m2 * rinv + temp * d2;
+        }
       }
-      const float kernel = (tl[0] * dx0 + tl[1] * dx1 + tl[2] * dx2) * (rinv2 * rinv2 * rinv);
-      p0 += dx0 * kernel;
-      p1 += dx1 * kernel;
-      p2 += dx2 * kernel;
-    }
-    if (++pk == P1) {
-      pk = 0;
-      if (++pj == P1) {
-        pj = 0;
-        ++pi;
-      }
+      a0 += (double)p0;
+      a1 += (double)p1;
+      a2 += (double)p2;
     }
   }
 }
@@ -623,7 +636,6 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
                                          const Seg* __restrict__ segs, double* sm, float4* s4,
                                          double* cheb, float* chebf, const double* stab,
                                          const float4* stab32) {
-  float* sf = reinterpret_cast<float*>(s4);  // proxy moments (FP32) share the tile buffer
   constexpr bool kCount = !MIXED;            // work counters come from the FP64 launches
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int blk = it.blk;
@@ -748,7 +760,6 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
     } else if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_DL_ON || KIND == K_DL_OFF) {
       constexpr bool DL = (KIND == K_DL_ON || KIND == K_DL_OFF);
       const int P1 = T.P1, Pf = T.Pf, C = T.C;
-      const int PT = (kSmem / C) & ~31;
       __syncthreads();
       if (tid < 3 * P1) {
         const double v = T.tcheb[(size_t)E.node * 3 * P1 + tid];
@@ -756,29 +767,42 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
         if (MIXED) chebf[tid] = (float)(v - cb[tid / P1]);
       }
       const double* M = T.mom + (size_t)E.node * C * Pf;
-      for (int kk0 = 0; kk0 < Pf; kk0 += PT) {
-        const int cnt = min(PT, Pf - kk0);
-        __syncthreads();
-        for (int c = 0; c < C; c++)
-          for (int i = tid; i < cnt; i += kTB) {
-            const double v = M[(size_t)c * Pf + kk0 + i];
-            if (MIXED) sf[c * PT + i] = (float)v;
-            else sm[c * PT + i] = v;
+      if (MIXED) {
+        // whole Chebyshev slabs per chunk, AoS float4 per proxy
+        constexpr int W = DL ? 3 : 2;
+        const int S2 = P1 * P1;
+        const int nsl = max(1, (3 * kNT / W) / S2);
+        for (int sl0 = 0; sl0 < P1; sl0 += nsl) {
+          const int ns = min(nsl, P1 - sl0);
+          const int kk0 = sl0 * S2, cnt = ns * S2;
+          __syncthreads();
+          float* f = reinterpret_cast<float*>(s4);
+          for (int e = tid; e < cnt * C; e += kTB) {
+            const int c = e / cnt, q = e - c * cnt;
+            f[q * 4 * W + c] = (float)M[(size_t)c * Pf + kk0 + q];
           }
-        __syncthreads();
-        if (wm != 0u && act) {
-          if (MIXED) {
-            for (int i0 = 0; i0 < cnt; i0 += 16) {
-              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-              proxies32<DL>(sf + i0, PT, min(16, cnt - i0), kk0 + i0, P1, chebf, F, p0, p1, p2);
-              a0 += (double)p0;
-              a1 += (double)p1;
-              a2 += (double)p2;
-            }
-          } else {
-            proxies64<DL>(sm, PT, cnt, kk0, P1, cheb, S, a0, a1, a2);
+          __syncthreads();
+          if (wm != 0u && act) proxies32_slabs<DL>(s4, ns, sl0, P1, chebf, F, a0, a1, a2);
+        }
+      }
+      if (!MIXED) {
+        // whole Chebyshev slabs per chunk, AoS double2 per proxy
+        constexpr int W = DL ? 6 : 3;
+        const int S2 = P1 * P1;
+        const int nsl = max(1, (kSmem / (2 * W)) / S2);
+        for (int sl0 = 0; sl0 < P1; sl0 += nsl) {
+          const int ns = min(nsl, P1 - sl0);
+          const int kk0 = sl0 * S2, cnt = ns * S2;
+          __syncthreads();
+          for (int e = tid; e < cnt * C; e += kTB) {
+            const int c = e / cnt, q = e - c * cnt;
+            sm[q * 2 * W + c] = M[(size_t)c * Pf + kk0 + q];
           }
-          if (kCount) cprox += cnt;
+          __syncthreads();
+          if (wm != 0u && act) {
+            proxies64_slabs<DL>(reinterpret_cast<const double2*>(sm), ns, sl0, P1, cheb, S, a0, a1, a2);
+            if (kCount) cprox += cnt;
+          }
         }
       }
     }
@@ -809,9 +833,9 @@ template <int FAM, bool MIXED>
 __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict__ tasks,
                                                       const BlockRef* __restrict__ items,
                                                       const Seg* __restrict__ segs) {
-  __shared__ double sm[kSmem];
+  __shared__ __align__(16) double sm[kSmem];
   // FP32 source tile: (x, y, z, area), (n, 0), (q, 0) per source; also holds
-  // FP32 proxy moments (kSmem floats at most)
+  // the FP32 proxy moments of whole Chebyshev slabs (3 or 2 float4 per proxy)
   __shared__ float4 sf[MIXED ? 3 * kNT : 1];
   __shared__ double cheb[3 * kMaxP1];
   __shared__ float chebf[3 * kMaxP1];
