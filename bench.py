@@ -33,6 +33,7 @@ sys.path.insert(0, os.path.join(ROOT, "high-order-regularization_b200"))
 
 H_INV = 64
 P, N0, THETA = 6, 2000, 0.6
+INNER = None  # (P, N0) of the inner treecode of the mixed solve's GMRES-IR cycles
 RESTART, TOL = 50, 1e-10
 
 
@@ -315,6 +316,21 @@ def run_ours(args, rank, world, local_rank):
         v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, args.steps, guess)
         v["features_host_ms"] = 1e3 * feat_s
         variants["mixed_warm"] = v
+    # GMRES-IR with the inner cycles on a treecode of their own (lower degree
+    # and leaf size); the FP64 true residuals keep the benchmark's treecode
+    ms_dl_inner = None
+    if INNER is not None:
+        plan.set_inner_tree(INNER[0], INNER[1], THETA)
+        for name, g in (("mixed_inner", None), ("mixed_inner_warm", guess)):
+            if name.endswith("warm") and g is None:
+                continue
+            timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, g)
+            v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, args.steps, g)
+            v["inner_tree"] = {"P": INNER[0], "N0": INNER[1], "theta": THETA}
+            variants[name] = v
+        plan.matvec_dev(x, b, highreg.HR_MIXED)
+        ms_dl_inner = plan.time_batch(3, 20)
+        plan.set_inner_tree(0, 0, THETA)
     for v in variants.values():
         v["speedup_vs_fp64"] = variants["fp64"]["ms_per_step"] / v["ms_per_step"]
     del guess  # releases the network before the context goes
@@ -340,8 +356,15 @@ def run_ours(args, rank, world, local_rank):
                 "frac": achieved / peak, "traffic": None,
                 "flops_per_launch": fl_launch, "ms_per_launch": ms_dl,
                 "ms_per_launch_mixed_precision": ms_dl_mixed,
+                "ms_per_launch_mixed_inner_tree": ms_dl_inner,
                 "peak_source": "measured FP64 FMA loop (hr_measure_fp64_peak) on this GPU",
                 "peak_fp32": peak32 / 1e12}
+    if H_INV == 64 and P == 6 and N0 == 2000:
+        # dram__bytes_read.sum + dram__bytes_write.sum of this launch from one ncu capture
+        # (profiles/eval_kernel_fp64_stresslet_h64.md): sources are staged once per tile, so
+        # DRAM traffic is tiny next to the compute; the bound is the FP64 pipe
+        roofline["traffic"] = 16364032 + 1024
+        roofline["traffic_source"] = "ncu capture of this kernel at this workload"
 
     # end to end through the C ABI with host buffers: scene upload + plan
     # (trees, interaction lists, stencils) + RHS + solve + solution read back
@@ -503,9 +526,18 @@ def main():
     ap.add_argument("--workload", default="2s", choices=["2s", "e2g"],
                     help="2s: the two-surface solve (the benchmark); e2g: the extend-to-grid pipeline")
     ap.add_argument("--N", type=int, default=96, help="extend-to-grid grid size (96 or 384)")
+    ap.add_argument("--inner", default="auto",
+                    help="treecode 'P,N0' of the mixed solve's inner operator; 'auto': 6,2000 when the "
+                         "workload's treecode is finer, 'none': no inner treecode")
     args = ap.parse_args()
-    global H_INV, P, N0
+    global H_INV, P, N0, INNER
     H_INV, P, N0 = args.h, args.P, args.N0
+    if args.inner == "auto":
+        INNER = (6, 2000) if (P, N0) != (6, 2000) and P >= 6 else None
+    elif args.inner == "none":
+        INNER = None
+    else:
+        INNER = tuple(int(v) for v in args.inner.split(","))
     rank, world, local_rank = dist_info()
     if world > 1:
         import datetime

@@ -102,17 +102,28 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(
   }
 }
 
-// Sums the partial moments of each node in item order (deterministic).
+// Sums the partial moments of each node in item order (deterministic) and
+// stores them proxy-major: FP64 C doubles per proxy, and an FP32 copy with W32
+// floats per proxy (12 for the stresslet's 12 channels, 8 for the Stokeslet's
+// 6 plus two zeros), so that a warp reads one proxy's moments as a few
+// contiguous vector loads.
 __global__ void moments_reduce_kernel(int C, int Pf, const int* __restrict__ item_start,
-                                      const double* __restrict__ partial, double* __restrict__ mom) {
+                                      const double* __restrict__ partial, double* __restrict__ mom,
+                                      float* __restrict__ momf) {
   const int node = blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int CP = C * Pf;
   if (i >= CP) return;
+  const int c = i / Pf, kk = i - c * Pf;
+  const int W32 = C == 12 ? 12 : 8;
   const int a = item_start[node], b = item_start[node + 1];
   double s = 0.0;
   for (int q = a; q < b; q++) s += partial[(size_t)q * CP + i];
-  mom[(size_t)node * CP + i] = (a < b) ? s : 0.0;
+  s = (a < b) ? s : 0.0;
+  mom[((size_t)node * Pf + kk) * C + c] = s;
+  float* f = momf + ((size_t)node * Pf + kk) * W32;
+  f[c] = (float)s;
+  if (C == 6 && c < 2) f[6 + c] = 0.f;
 }
 
 __global__ void permute_kernel(int n, const int* __restrict__ perm, const double* __restrict__ q3,
@@ -313,10 +324,10 @@ void launch_moments(int dl, const MomItem* d_items, int nitems, int P1, const do
 }
 
 void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_start,
-                           const double* partial, double* mom, cudaStream_t st) {
+                           const double* partial, double* mom, float* momf, cudaStream_t st) {
   if (nnodes_out <= 0) return;
   dim3 grid((C * Pf + 255) / 256, nnodes_out);
-  moments_reduce_kernel<<<grid, 256, 0, st>>>(C, Pf, d_item_start, partial, mom);
+  moments_reduce_kernel<<<grid, 256, 0, st>>>(C, Pf, d_item_start, partial, mom, momf);
 }
 
 void launch_permute(int n, const int* perm, const double* q3, double* qx, double* qy, double* qz,

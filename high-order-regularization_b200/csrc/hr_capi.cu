@@ -413,41 +413,65 @@ struct hr_plan2s {
   // GMRES work space
   int Vcols = 0;
   DBuf<double> V, r, bsave, partial, hbuf, ybuf;
+  // Optional treecode of the reduced-precision inner operator of GMRES-IR:
+  // trees and interaction lists of its own over the same targets, stencils
+  // and output buffers.
+  struct Inner {
+    int P = 0, N0 = 0;
+    double theta = 0.0;
+    DevTree tree[2];
+    DevLists Lon[2], Loff[2];
+    Batch dl[3];  // [1] mixed, [2] all FP32 ([0] unused)
+  };
+  std::unique_ptr<Inner> inner;
+  // host copies of the surfaces and near flags, for building an inner treecode later
+  std::vector<double> hxyz[2], hnrml[2], harea[2];
+  std::vector<uint8_t> near_host[2];
+  hr_surface surf_host[2];
 };
 
 namespace {
 
-void plan_batches(hr_plan2s& P) {
+// Stresslet batches of the matvec, one per precision from prec0 on, over the
+// given trees and lists (the plan's own, or the inner operator's).
+void dl_batches(hr_plan2s& P, DevTree* tree, DevLists* Lon, DevLists* Loff, Batch* dl, int prec0,
+                bool count) {
   cudaStream_t st = P.C->stream;
   const bool direct = P.opt.mode == HR_DIRECT;
-  P.counters.alloc(4 * 8);
-  P.counters.zero(st);
-  for (int prec = 0; prec < 3; prec++) {
-    Batch& B = P.dl[prec];
+  for (int prec = prec0; prec < 3; prec++) {
+    Batch& B = dl[prec];
     B.family = F_DL;
     B.tasks.clear();
     B.lists.clear();
+    B.trees.clear();
     for (int t = 0; t < 2; t++) {
       const int s = t;
       EvalTask on = make_task(K_DL_ON, P.delta, direct ? dl_scale_direct() : dl_scale_tree(),
-                              P.tree[s], P.Lon[t], P.tg[t], P.out_on[t].p);
+                              tree[s], Lon[t], P.tg[t], P.out_on[t].p);
       on.tq = P.xin.p + P.off[s];
       on.mixed = prec;
-      on.counters = P.counters.p + 4 * (2 * t);
+      if (count) on.counters = P.counters.p + 4 * (2 * t);
       EvalTask of = make_task(K_DL_OFF, P.delta, direct ? dl_scale_direct() : dl_scale_tree(),
-                              P.tree[1 - t], P.Loff[t], P.tg[t], P.out_off[t].p);
+                              tree[1 - t], Loff[t], P.tg[t], P.out_off[t].p);
       of.jump_mode = direct ? 1 : 0;
       of.mixed = prec;
-      of.counters = P.counters.p + 4 * (2 * t + 1);
+      if (count) of.counters = P.counters.p + 4 * (2 * t + 1);
       B.tasks.push_back(on);
-      B.lists.push_back(&P.Lon[t].host);
-      B.trees.push_back(&P.tree[s].host);
+      B.lists.push_back(&Lon[t].host);
+      B.trees.push_back(&tree[s].host);
       B.tasks.push_back(of);
-      B.lists.push_back(&P.Loff[t].host);
-      B.trees.push_back(&P.tree[1 - t].host);
+      B.lists.push_back(&Loff[t].host);
+      B.trees.push_back(&tree[1 - t].host);
     }
     B.finalize(st, P.C->num_sms);
   }
+}
+
+void plan_batches(hr_plan2s& P) {
+  cudaStream_t st = P.C->stream;
+  P.counters.alloc(4 * 8);
+  P.counters.zero(st);
+  dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, true);
   Batch& B = P.sl;
   B.family = F_SL;
   for (int t = 0; t < 2; t++) {
@@ -473,14 +497,17 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
   const bool tree = P.opt.mode == HR_TREE;
   if (x_dev != P.xin.p)
     HR_CHECK_CUDA(cudaMemcpyAsync(P.xin.p, x_dev, sizeof(double) * P.n, cudaMemcpyDeviceToDevice, st));
-  for (int s = 0; s < 2; s++) P.tree[s].set_density(C, P.xin.p + P.off[s], true, tree, prec != HR_FP64);
+  // the reduced-precision operator runs on the inner treecode when there is one
+  hr_plan2s::Inner* in = (prec != HR_FP64 && P.inner) ? P.inner.get() : nullptr;
+  DevTree* trees = in ? in->tree : P.tree;
+  for (int s = 0; s < 2; s++) trees[s].set_density(C, P.xin.p + P.off[s], true, tree, prec != HR_FP64);
   for (int t = 0; t < 2; t++) {
     P.tg[t].g0.zero(st);
     launch_interp(P.sten[t].ne, P.sten[t].tgt.p, P.sten[t].idx.p, P.sten[t].pq.p,
                   P.xin.p + P.off[1 - t], P.tg[t].g0.p, st);
     C.launches++;
   }
-  P.dl[prec].launch(C);
+  (in ? in->dl[prec] : P.dl[prec]).launch(C);
   // set 0: u - on*f - comp*f ; set 1: u - comp*f - on*f   (2S/main.cpp:612-676)
   launch_matvec_combine(3 * P.nq[0], 2.0 / 3.0, P.xin.p + P.off[0], P.out_on[0].p, P.out_off[0].p,
                         y_dev + P.off[0], st);
@@ -555,10 +582,15 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
   double b_norm = dev_norm(P, b_dev);
   double bscale = b_norm > 1.e-8 ? b_norm : 1.0;
   double* r = P.r.p;
-  // initial residual
+  // initial residual; with refinement the guess's residual comes from the
+  // reduced-precision operator (the first FP64 true residual follows its cycle)
+  bool r_true = true;  // r holds the FP64 residual b - A x
   if (o.use_guess) {
-    plan_matvec(P, x_dev, r, 0);
-    R.matvecs_fp64++;
+    const int p0 = refine ? o.precision : HR_FP64;
+    plan_matvec(P, x_dev, r, p0);
+    if (p0) R.matvecs_mixed++;
+    else R.matvecs_fp64++;
+    r_true = p0 == HR_FP64;
     launch_sub(n, b_dev, r, r, st);
     C.launches++;
     double rn = dev_norm(P, r);
@@ -567,6 +599,7 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
       HR_CHECK_CUDA(cudaMemsetAsync(x_dev, 0, sizeof(double) * n, st));
       launch_copy(n, b_dev, r, st);
       C.launches++;
+      r_true = true;
     }
   } else {
     HR_CHECK_CUDA(cudaMemsetAsync(x_dev, 0, sizeof(double) * n, st));
@@ -589,6 +622,15 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
       break;
     }
     if (refine && R.restarts > 0) R.true_residual = error;
+    if (error <= o.tol && !r_true) {  // a guess already good enough: confirm in FP64
+      plan_matvec(P, x_dev, r, 0);
+      R.matvecs_fp64++;
+      launch_sub(n, b_dev, r, r, st);
+      C.launches++;
+      r_true = true;
+      R.restarts++;
+      continue;
+    }
     if (error <= o.tol || iter >= max_iter) break;
     const double err_start = error;
     const double cycle_tol = (refine && !fp64_tail) ? std::max(0.5 * o.tol, eta * err_start) : o.tol;
@@ -666,6 +708,7 @@ int plan_solve(hr_plan2s& P, const hr_gmres_opts& o, const double* b_dev, double
     R.matvecs_fp64++;
     launch_sub(n, b_dev, r, r, st);
     C.launches++;
+    r_true = true;
     if (refine) {
       const double tr = dev_norm(P, r) / bscale;
       if (!(tr <= 0.5 * err_start)) fp64_tail = 1;  // the reduced-precision cycle stalled
@@ -728,6 +771,15 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
       check_finite(S.nrml, 3 * (size_t)S.n, "surface normals");
       check_finite(S.area, S.n, "area weights");
       P->nq[s] = S.n;
+      P->hxyz[s].assign(S.xyz, S.xyz + 3 * (size_t)S.n);
+      P->hnrml[s].assign(S.nrml, S.nrml + 3 * (size_t)S.n);
+      P->harea[s].assign(S.area, S.area + S.n);
+      hr_surface& H = P->surf_host[s];
+      H = S;
+      H.xyz = P->hxyz[s].data();
+      H.nrml = P->hnrml[s].data();
+      H.area = P->harea[s].data();
+      H.plane = nullptr;
     }
     P->off[0] = 0;
     P->off[1] = 3 * P->nq[0];
@@ -737,6 +789,7 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
     for (int t = 0; t < 2; t++) {
       const hr_targets& T = sc->tgt[t];
       std::vector<uint8_t> near = near_flags(T.n, T.b, sc->delta);
+      P->near_host[t] = near;
       upload_targets(P->tg[t], T.n, sc->surf[t].xyz, T.b, T.x0, T.n0, sc->f0[t], sc->surf[t].nrml,
                      near, st);
       std::vector<uint8_t> all(T.n, 1);
@@ -766,6 +819,37 @@ extern "C" void hr_plan2s_destroy(hr_plan2s* plan) {
   if (!plan) return;
   if (plan->C) cudaStreamSynchronize(plan->C->stream);
   delete plan;
+}
+
+extern "C" int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double theta) {
+  if (!plan) return HR_ERR_ARG;
+  return guard(plan->owner, [&] {
+    hr_plan2s& Q = *plan;
+    HR_REQUIRE(Q.opt.mode == HR_TREE, "an inner treecode needs an HR_TREE plan");
+    if (P == 0) {
+      HR_CHECK_CUDA(cudaStreamSynchronize(Q.C->stream));
+      Q.inner.reset();
+      return;
+    }
+    HR_REQUIRE(P >= 1 && P <= 15, "inner treecode degree P must be in [1, 15]");
+    HR_REQUIRE(N0 >= 1, "inner treecode leaf size N0 must be >= 1");
+    HR_REQUIRE(theta > 0.0 && theta < 1.0, "inner treecode theta must be in (0, 1)");
+    cudaStream_t st = Q.C->stream;
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+    std::unique_ptr<hr_plan2s::Inner> in(new hr_plan2s::Inner);
+    in->P = P;
+    in->N0 = N0;
+    in->theta = theta;
+    for (int s = 0; s < 2; s++) in->tree[s].build(Q.surf_host[s], P, N0, theta, false, st);
+    for (int t = 0; t < 2; t++) {
+      std::vector<uint8_t> all(Q.nq[t], 1);
+      in->Lon[t].build(in->tree[t].host, Q.nq[t], Q.surf_host[t].xyz, all.data(), st);
+      in->Loff[t].build(in->tree[1 - t].host, Q.nq[t], Q.surf_host[t].xyz, Q.near_host[t].data(), st);
+    }
+    dl_batches(Q, in->tree, in->Lon, in->Loff, in->dl, 1, false);
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+    Q.inner = std::move(in);
+  });
 }
 
 extern "C" void* hr_plan2s_stream(hr_plan2s* plan) { return plan ? (void*)plan->C->stream : nullptr; }
@@ -949,12 +1033,12 @@ extern "C" int hr_plan2s_check_upward_pass(hr_plan2s* plan, const double* x, dou
       // per node and channel, relative to that channel's largest FP64 moment
       for (int nd = 0; nd < T.nn; nd++)
         for (int c = 0; c < 12; c++) {
-          const double* pa = a.data() + ((size_t)nd * 12 + c) * T.Pf;
-          const double* pb = b.data() + ((size_t)nd * 12 + c) * T.Pf;
+          const double* pa = a.data() + (size_t)nd * 12 * T.Pf + c;
+          const double* pb = b.data() + (size_t)nd * 12 * T.Pf + c;
           double mx = 0.0, dif = 0.0;
           for (int k = 0; k < T.Pf; k++) {
-            mx = std::max(mx, fabs(pa[k]));
-            dif = std::max(dif, fabs(pa[k] - pb[k]));
+            mx = std::max(mx, fabs(pa[12 * k]));
+            dif = std::max(dif, fabs(pa[12 * k] - pb[12 * k]));
           }
           if (mx > 0.0) worst = std::max(worst, dif / mx);
         }
@@ -992,10 +1076,11 @@ extern "C" int hr_measure_fp32_peak(hr_ctx* ctx, double* flops_per_s) {
 }
 
 extern "C" int hr_plan2s_time_batch(hr_plan2s* plan, int which, int iters, double* ms_per_launch) {
-  if (!plan || !ms_per_launch || iters < 1 || which < 0 || which > 2) return HR_ERR_ARG;
+  if (!plan || !ms_per_launch || iters < 1 || which < 0 || which > 3) return HR_ERR_ARG;
   return guard(ctx_of(plan), [&] {
     cudaStream_t st = plan->C->stream;
-    Batch& B = which == 1 ? plan->sl : plan->dl[which == 2 ? 1 : 0];
+    HR_REQUIRE(which != 3 || plan->inner, "the plan has no inner treecode");
+    Batch& B = which == 3 ? plan->inner->dl[1] : which == 1 ? plan->sl : plan->dl[which == 2 ? 1 : 0];
     cudaEvent_t a, b;
     HR_CHECK_CUDA(cudaEventCreate(&a));
     HR_CHECK_CUDA(cudaEventCreate(&b));

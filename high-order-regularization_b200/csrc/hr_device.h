@@ -27,7 +27,8 @@ struct EvalTask {
   const float *fx, *fy, *fz, *fnx, *fny, *fnz, *fa, *fqx, *fqy, *fqz;
   const int *node_m0, *node_m1;                       // inclusive member ranges
   const double* tcheb;                                // 3*P1 per node
-  const double* mom;                                  // C*Pf per node
+  const double* mom;                                  // Pf*C per node, proxy-major
+  const float* momf;                                  // Pf*W32 per node (W32 = 12 DL, 8 SL)
   const int* tord;                                    // target order -> target index
   const double* txyz;                                 // 3nt targets
   const double* tb;                                   // nt signed distances
@@ -96,7 +97,7 @@ void launch_moments(int dl, const MomItem* d_items, int nitems, int P1, const do
                     const double* ny, const double* nz, const double* a, const double* qx,
                     const double* qy, const double* qz, double* partial, cudaStream_t st);
 void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_start,
-                           const double* partial, double* mom, cudaStream_t st);
+                           const double* partial, double* mom, float* momf, cudaStream_t st);
 
 // Gathers interleaved reference-order density into tree-order SoA.
 void launch_permute(int n, const int* perm, const double* q3, double* qx, double* qy, double* qz,

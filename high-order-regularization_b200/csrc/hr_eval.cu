@@ -71,8 +71,10 @@ __device__ __forceinline__ double smooth_eval(const double* __restrict__ tab, do
   return v;
 }
 
-constexpr int kNT = 256;         // sources per shared-memory tile
-constexpr int kSmem = 10 * kNT;  // doubles: 10 SoA arrays of a source tile
+constexpr int kWarps = kTB / 32;     // warps per CTA, each with its own tiles
+constexpr int kNT = 64;              // sources per (per-warp) shared-memory tile
+constexpr int kWarpSm = 10 * kNT;    // doubles per warp: 10 SoA arrays of a source tile
+constexpr int kSmem = kWarps * kWarpSm;
 constexpr int kMaxP1 = 16;
 
 struct Tgt {
@@ -526,108 +528,115 @@ __device__ __forceinline__ bool pair32r(const float4* __restrict__ s4, int j, co
 
 
 
-// FP64 proxy interactions of whole Chebyshev slabs: as proxies32_slabs with
-// the moments staged per proxy as double2 (DL: 6, SL: 3 per proxy, channel
-// order as in the moment array) and FP64 arithmetic throughout.
+// Asynchronous copy of `bytes` (a multiple of 16, both addresses 16-byte
+// aligned) from global to shared memory by the 32 lanes of a warp.
+__device__ __forceinline__ void warp_copy_async(void* dst, const void* src, int bytes, int lane) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  const char* s = static_cast<const char*>(src);
+  for (int o = lane * 16; o < bytes; o += 32 * 16)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d + o), "l"(s + o) : "memory");
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void copy_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Proxy interactions of a run of Chebyshev rows (row r = i (P+1) + j holds
+// proxies (i, j, 0..P)) from the warp's shared copy of the node's proxy-major
+// moments: FP64 as double2 (DL 6, SL 3 per proxy), FP32 as float4 (DL: M00
+// M01 M02 M10 | M11 M12 M20 M21 | M22 Mn0 Mn1 Mn2; SL: f0 f1 f2 n0 | n1 n2 - -).
+// Every lane reads the same proxy (a shared-memory broadcast). The stresslet
+// kernel uses
+//   sum_l (sum_k (M[3l+k] - g0_l Mn_k) d_k) d_l = d.M.d - (g0.d)(Mn.d),
+// the reference's proxy sum (Call_Treecode_DL, 2S/KITC.cpp:753-771)
+// regrouped; Call_Treecode_SL (2S/KITC.cpp:700-714) as written.
 template <bool DL>
-__device__ __forceinline__ void proxies64_slabs(const double2* __restrict__ s2, int nslab, int pi0, int P1,
-                                                const double* __restrict__ cheb, const Tgt& S, double& a0,
-                                                double& a1, double& a2) {
+__device__ __forceinline__ void proxies64_rows(const double2* __restrict__ s2, int row0, int nrows, int P1,
+                                               const double* __restrict__ cheb, const Tgt& S, double& a0,
+                                               double& a1, double& a2) {
   constexpr int W = DL ? 6 : 3;  // double2 per proxy
-  const int S2 = P1 * P1;
-  for (int sl = 0; sl < nslab; sl++) {
-    const double d0 = S.px - cheb[pi0 + sl];
-    const double2* slab = s2 + sl * S2 * W;
-    for (int pj = 0; pj < P1; pj++) {
-      const double d1 = S.py - cheb[P1 + pj];
-      const double r01 = d0 * d0 + d1 * d1;
-      const double2* row = slab + pj * P1 * W;
-      for (int pk = 0; pk < P1; pk++) {
-        const double d2 = S.pz - cheb[2 * P1 + pk];
-        const double rinv = rsqrt(fma(d2, d2, r01));
-        const double2* m = row + pk * W;
-        if (DL) {
-          const double2 m01 = m[0], m23 = m[1], m45 = m[2], m67 = m[3], m89 = m[4], m1011 = m[5];
-          const double u0 = m01.x * d0 + m01.y * d1 + m23.x * d2;
-          const double u1 = m23.y * d0 + m45.x * d1 + m45.y * d2;
-          const double u2 = m67.x * d0 + m67.y * d1 + m89.x * d2;
-          const double dmd = d0 * u0 + d1 * u1 + d2 * u2;
-          const double mnd = m89.y * d0 + m1011.x * d1 + m1011.y * d2;
-          const double g0d = S.g0[0] * d0 + S.g0[1] * d1 + S.g0[2] * d2;
-          const double ri2 = rinv * rinv;
-          const double kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
-          a0 += d0 * kernel;
-          a1 += d1 * kernel;
-          a2 += d2 * kernel;
-        } else {
-          const double2 m01 = m[0], m23 = m[1], m45 = m[2];
-          const double q0 = m01.x - S.f0n0 * m23.y;
-          const double q1 = m01.y - S.f0n0 * m45.x;
-          const double q2 = m23.x - S.f0n0 * m45.y;
-          const double temp = (q0 * d0 + q1 * d1 + q2 * d2) * (rinv * rinv * rinv);
-          a0 += q0 * rinv + temp * d0;
-          a1 += q1 * rinv + temp * d1;
-          a2 += q2 * rinv + temp * d2;
-        }
+  for (int r = 0; r < nrows; r++) {
+    const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
+    const double d0 = S.px - cheb[pi];
+    const double d1 = S.py - cheb[P1 + pj];
+    const double r01 = d0 * d0 + d1 * d1;
+    const double2* row = s2 + r * P1 * W;
+    for (int pk = 0; pk < P1; pk++) {
+      const double d2 = S.pz - cheb[2 * P1 + pk];
+      const double rinv = rsqrt(fma(d2, d2, r01));
+      const double2* m = row + pk * W;
+      if (DL) {
+        const double2 m01 = m[0], m23 = m[1], m45 = m[2], m67 = m[3], m89 = m[4], m1011 = m[5];
+        const double u0 = m01.x * d0 + m01.y * d1 + m23.x * d2;
+        const double u1 = m23.y * d0 + m45.x * d1 + m45.y * d2;
+        const double u2 = m67.x * d0 + m67.y * d1 + m89.x * d2;
+        const double dmd = d0 * u0 + d1 * u1 + d2 * u2;
+        const double mnd = m89.y * d0 + m1011.x * d1 + m1011.y * d2;
+        const double g0d = S.g0[0] * d0 + S.g0[1] * d1 + S.g0[2] * d2;
+        const double ri2 = rinv * rinv;
+        const double kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
+        a0 += d0 * kernel;
+        a1 += d1 * kernel;
+        a2 += d2 * kernel;
+      } else {
+        const double2 m01 = m[0], m23 = m[1], m45 = m[2];
+        const double q0 = m01.x - S.f0n0 * m23.y;
+        const double q1 = m01.y - S.f0n0 * m45.x;
+        const double q2 = m23.x - S.f0n0 * m45.y;
+        const double temp = (q0 * d0 + q1 * d1 + q2 * d2) * (rinv * rinv * rinv);
+        a0 += q0 * rinv + temp * d0;
+        a1 += q1 * rinv + temp * d1;
+        a2 += q2 * rinv + temp * d2;
       }
     }
   }
 }
 
-// FP32 proxy interactions of whole Chebyshev slabs (fixed first index i):
-// nslab slabs starting at i = pi0, moments staged per proxy as float4
-// (DL: M00 M01 M02 M10 | M11 M12 M20 M21 | M22 Mn0 Mn1 Mn2; SL: f0 f1 f2 n0 |
-// n1 n2 - -), proxies of a slab in (j, k) order. The stresslet kernel uses
-//   sum_l (sum_k (M[3l+k] - g0_l Mn_k) d_k) d_l = d.M.d - (g0.d)(Mn.d),
-// the reference's proxy sum (Call_Treecode_DL, 2S/KITC.cpp:753-771)
-// regrouped; Call_Treecode_SL (2S/KITC.cpp:700-714) as written. Partial sums
-// of one (i, j) row go to the FP64 accumulators.
+// FP32 proxies, FP64 accumulation per Chebyshev row.
 template <bool DL>
-__device__ __forceinline__ void proxies32_slabs(const float4* __restrict__ s4, int nslab, int pi0, int P1,
-                                                const float* __restrict__ chebf, const Tgt32& F, double& a0,
-                                                double& a1, double& a2) {
+__device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, int row0, int nrows, int P1,
+                                               const float* __restrict__ chebf, const Tgt32& F, double& a0,
+                                               double& a1, double& a2) {
   constexpr int W = DL ? 3 : 2;  // float4 per proxy
-  const int S2 = P1 * P1;
-  for (int sl = 0; sl < nslab; sl++) {
-    const float d0 = F.px - chebf[pi0 + sl];
-    const float4* slab = s4 + sl * S2 * W;
-    for (int pj = 0; pj < P1; pj++) {
-      const float d1 = F.py - chebf[P1 + pj];
-      const float r01 = d0 * d0 + d1 * d1;
-      const float4* row = slab + pj * P1 * W;
-      float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-      for (int pk = 0; pk < P1; pk++) {
-        const float d2 = F.pz - chebf[2 * P1 + pk];
-        const float rinv = rsqrtf(fmaf(d2, d2, r01));
-        const float4 A = row[pk * W];
-        const float4 B = row[pk * W + 1];
-        if (DL) {
-          const float4 Cc = row[pk * W + 2];
-          const float u0 = A.x * d0 + A.y * d1 + A.z * d2;
-          const float u1 = A.w * d0 + B.x * d1 + B.y * d2;
-          const float u2 = B.z * d0 + B.w * d1 + Cc.x * d2;
-          const float dmd = d0 * u0 + d1 * u1 + d2 * u2;
-          const float mnd = Cc.y * d0 + Cc.z * d1 + Cc.w * d2;
-          const float g0d = F.g0[0] * d0 + F.g0[1] * d1 + F.g0[2] * d2;
-          const float ri2 = rinv * rinv;
-          const float kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
-          p0 += d0 * kernel;
-          p1 += d1 * kernel;
-          p2 += d2 * kernel;
-        } else {
-          const float m0 = A.x - F.f0n0 * A.w;
-          const float m1 = A.y - F.f0n0 * B.x;
-          const float m2 = A.z - F.f0n0 * B.y;
-          const float temp = (m0 * d0 + m1 * d1 + m2 * d2) * (rinv * rinv * rinv);
-          p0 += m0 * rinv + temp * d0;
-          p1 += m1 * rinv + temp * d1;
-          p2 += m2 * rinv + temp * d2;
-        }
+  for (int r = 0; r < nrows; r++) {
+    const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
+    const float d0 = F.px - chebf[pi];
+    const float d1 = F.py - chebf[P1 + pj];
+    const float r01 = d0 * d0 + d1 * d1;
+    const float4* row = s4 + r * P1 * W;
+    float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+    for (int pk = 0; pk < P1; pk++) {
+      const float d2 = F.pz - chebf[2 * P1 + pk];
+      const float rinv = rsqrtf(fmaf(d2, d2, r01));
+      const float4 A = row[pk * W];
+      const float4 B = row[pk * W + 1];
+      if (DL) {
+        const float4 Cc = row[pk * W + 2];
+        const float u0 = A.x * d0 + A.y * d1 + A.z * d2;
+        const float u1 = A.w * d0 + B.x * d1 + B.y * d2;
+        const float u2 = B.z * d0 + B.w * d1 + Cc.x * d2;
+        const float dmd = d0 * u0 + d1 * u1 + d2 * u2;
+        const float mnd = Cc.y * d0 + Cc.z * d1 + Cc.w * d2;
+        const float g0d = F.g0[0] * d0 + F.g0[1] * d1 + F.g0[2] * d2;
+        const float ri2 = rinv * rinv;
+        const float kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
+        p0 += d0 * kernel;
+        p1 += d1 * kernel;
+        p2 += d2 * kernel;
+      } else {
+        const float m0 = A.x - F.f0n0 * A.w;
+        const float m1 = A.y - F.f0n0 * B.x;
+        const float m2 = A.z - F.f0n0 * B.y;
+        const float temp = (m0 * d0 + m1 * d1 + m2 * d2) * (rinv * rinv * rinv);
+        p0 += m0 * rinv + temp * d0;
+        p1 += m1 * rinv + temp * d1;
+        p2 += m2 * rinv + temp * d2;
       }
-      a0 += (double)p0;
-      a1 += (double)p1;
-      a2 += (double)p2;
     }
+    a0 += (double)p0;
+    a1 += (double)p1;
+    a2 += (double)p2;
   }
 }
 
@@ -674,85 +683,92 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
                                    KIND == K_E2G_SL7 || KIND == K_E2G_P7);
   const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY ||
                                ((KIND == K_SL_OFF || KIND == K_DL_OFF) && !S.near));
+  // Each warp walks the item's segments on its own: its own source tiles in
+  // shared memory, __syncwarp only, and an entry whose mask is zero for this
+  // warp is skipped outright.
+  double* wsm = sm + warp * kWarpSm;
+  float4* ws4 = s4 + warp * 3 * kNT;
+  double* wcheb = cheb + warp * 3 * kMaxP1;
+  float* wchebf = chebf + warp * 3 * kMaxP1;
   for (int q = it.seg0; q < it.seg1; q++) {
     const Seg sg = segs[q];
     const Entry E = T.entries[sg.entry];
     const uint32_t wm = E.mask[warp];
+    if (wm == 0u) continue;
     const bool act = valid && ((wm >> lane) & 1u);
     if (E.type == 1) {
       const int m0 = sg.s0, m1 = sg.s1 - 1;
       for (int s0 = m0; s0 <= m1; s0 += kNT) {
         const int cnt = min(kNT, m1 - s0 + 1);
-        __syncthreads();
-        for (int i = tid; i < cnt; i += kTB) {
+        __syncwarp();
+        for (int i = lane; i < cnt; i += 32) {
           const int s = s0 + i;
           const double x = T.sx[s], y = T.sy[s], z = T.sz[s];
           if (!kOn32) {
-            sm[i] = x;
-            sm[kNT + i] = y;
-            sm[2 * kNT + i] = z;
+            wsm[i] = x;
+            wsm[kNT + i] = y;
+            wsm[2 * kNT + i] = z;
             if (kSrcNrm) {
-              sm[3 * kNT + i] = T.snx[s];
-              sm[4 * kNT + i] = T.sny[s];
-              sm[5 * kNT + i] = T.snz[s];
+              wsm[3 * kNT + i] = T.snx[s];
+              wsm[4 * kNT + i] = T.sny[s];
+              wsm[5 * kNT + i] = T.snz[s];
             }
-            sm[6 * kNT + i] = T.sa[s];
-            sm[7 * kNT + i] = T.qx[s];
-            sm[8 * kNT + i] = T.qy[s];
-            sm[9 * kNT + i] = T.qz[s];
+            wsm[6 * kNT + i] = T.sa[s];
+            wsm[7 * kNT + i] = T.qx[s];
+            wsm[8 * kNT + i] = T.qy[s];
+            wsm[9 * kNT + i] = T.qz[s];
           }
           if (MIXED) {
-            s4[i] = make_float4((float)(x - cb[0]), (float)(y - cb[1]), (float)(z - cb[2]), T.fa[s]);
-            if (kSrcNrm) s4[kNT + i] = make_float4(T.fnx[s], T.fny[s], T.fnz[s], 0.f);
-            s4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
+            ws4[i] = make_float4((float)(x - cb[0]), (float)(y - cb[1]), (float)(z - cb[2]), T.fa[s]);
+            if (kSrcNrm) ws4[kNT + i] = make_float4(T.fnx[s], T.fny[s], T.fnz[s], 0.f);
+            ws4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
           }
         }
-        __syncthreads();
-        if (wm != 0u && act) {
-          if (kOn32) {
-            for (int j0 = 0; j0 < cnt; j0 += 16) {
-              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-              const int j1 = min(cnt, j0 + 16);
+        __syncwarp();
+        if (!act) continue;
+        if (kOn32) {
+          for (int j0 = 0; j0 < cnt; j0 += 16) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+            const int j1 = min(cnt, j0 + 16);
 #pragma unroll 4
-              for (int j = j0; j < j1; j++) pair32tab<KIND>(s4, j, F, gf, stab32, p0, p1, p2);
-              a0 += (double)p0;
-              a1 += (double)p1;
-              a2 += (double)p2;
+            for (int j = j0; j < j1; j++) pair32tab<KIND>(ws4, j, F, gf, stab32, p0, p1, p2);
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
+          }
+        } else if (all32) {
+          for (int j0 = 0; j0 < cnt; j0 += 16) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+            const int j1 = min(cnt, j0 + 16);
+            for (int j = j0; j < j1; j++) pair32<KIND>(ws4, j, F, p0, p1, p2);
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
+          }
+        } else if (MIXED && kPerPairSplit && S.near) {
+          for (int j0 = 0; j0 < cnt; j0 += 16) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f;
+            const int j1 = min(cnt, j0 + 16);
+            for (int j = j0; j < j1; j++) {
+              const float4 Pj = ws4[j];
+              const float dx = F.px - Pj.x, dy = F.py - Pj.y, dz = F.pz - Pj.z;
+              if (dx * dx + dy * dy + dz * dz > cut2f) pair32r<KIND>(ws4, j, F, gf, p0, p1, p2);
+              else pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
             }
-          } else if (all32) {
-            for (int j0 = 0; j0 < cnt; j0 += 16) {
-              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-              const int j1 = min(cnt, j0 + 16);
-              for (int j = j0; j < j1; j++) pair32<KIND>(s4, j, F, p0, p1, p2);
-              a0 += (double)p0;
-              a1 += (double)p1;
-              a2 += (double)p2;
-            }
-          } else if (MIXED && kPerPairSplit && S.near) {
-            for (int j0 = 0; j0 < cnt; j0 += 16) {
-              float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-              const int j1 = min(cnt, j0 + 16);
-              for (int j = j0; j < j1; j++) {
-                const float4 Pj = s4[j];
-                const float dx = F.px - Pj.x, dy = F.py - Pj.y, dz = F.pz - Pj.z;
-                if (dx * dx + dy * dy + dz * dz > cut2f) pair32r<KIND>(s4, j, F, gf, p0, p1, p2);
-                else pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
-              }
-              a0 += (double)p0;
-              a1 += (double)p1;
-              a2 += (double)p2;
-            }
-          } else {
-            unsigned cr = 0;
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
+          }
+        } else {
+          unsigned cr = 0;
 #pragma unroll 2
-            for (int j = 0; j < cnt; j++) cr += pair64<KIND>(sm, j, S, g, stab, a0, a1, a2);
-            if (kCount) {
-              if (S.near) {
-                creg += cr;
-                cplain += cnt - cr;
-              } else {
-                cfar += cnt;
-              }
+          for (int j = 0; j < cnt; j++) cr += pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
+          if (kCount) {
+            if (S.near) {
+              creg += cr;
+              cplain += cnt - cr;
+            } else {
+              cfar += cnt;
             }
           }
         }
@@ -760,51 +776,46 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
     } else if (KIND == K_SL_ON || KIND == K_SL_OFF || KIND == K_DL_ON || KIND == K_DL_OFF) {
       constexpr bool DL = (KIND == K_DL_ON || KIND == K_DL_OFF);
       const int P1 = T.P1, Pf = T.Pf, C = T.C;
-      __syncthreads();
-      if (tid < 3 * P1) {
-        const double v = T.tcheb[(size_t)E.node * 3 * P1 + tid];
-        cheb[tid] = v;
-        if (MIXED) chebf[tid] = (float)(v - cb[tid / P1]);
+      // The node's proxy-major moments stream through the warp's tile in
+      // runs of whole Chebyshev rows, double-buffered: the asynchronous copy
+      // of the next run overlaps the interactions of this one.
+      constexpr int kBpp = MIXED ? (DL ? 48 : 32) : (DL ? 96 : 48);  // bytes per proxy
+      constexpr int kHalf = kWarpSm * 4;                              // bytes per buffer
+      const char* src = MIXED ? reinterpret_cast<const char*>(T.momf + (size_t)E.node * Pf * (DL ? 12 : 8))
+                              : reinterpret_cast<const char*>(T.mom + (size_t)E.node * Pf * C);
+      char* buf = reinterpret_cast<char*>(wsm);
+      const int rowb = P1 * kBpp;
+      const int nr = max(1, kHalf / rowb);
+      const int nrow_all = P1 * P1;
+      const int nch = (nrow_all + nr - 1) / nr;
+      __syncwarp();
+      for (int i = lane; i < 3 * P1; i += 32) {
+        const double v = T.tcheb[(size_t)E.node * 3 * P1 + i];
+        wcheb[i] = v;
+        if (MIXED) wchebf[i] = (float)(v - cb[i / P1]);
       }
-      const double* M = T.mom + (size_t)E.node * C * Pf;
-      if (MIXED) {
-        // whole Chebyshev slabs per chunk, AoS float4 per proxy
-        constexpr int W = DL ? 3 : 2;
-        const int S2 = P1 * P1;
-        const int nsl = max(1, (3 * kNT / W) / S2);
-        for (int sl0 = 0; sl0 < P1; sl0 += nsl) {
-          const int ns = min(nsl, P1 - sl0);
-          const int kk0 = sl0 * S2, cnt = ns * S2;
-          __syncthreads();
-          float* f = reinterpret_cast<float*>(s4);
-          for (int e = tid; e < cnt * C; e += kTB) {
-            const int c = e / cnt, q = e - c * cnt;
-            f[q * 4 * W + c] = (float)M[(size_t)c * Pf + kk0 + q];
-          }
-          __syncthreads();
-          if (wm != 0u && act) proxies32_slabs<DL>(s4, ns, sl0, P1, chebf, F, a0, a1, a2);
+      warp_copy_async(buf, src, min(nr, nrow_all) * rowb, lane);
+      for (int ch = 0; ch < nch; ch++) {
+        const int row0 = ch * nr, rows = min(nr, nrow_all - row0);
+        if (ch + 1 < nch) {
+          const int r1 = row0 + nr;
+          warp_copy_async(buf + ((ch + 1) & 1) * kHalf, src + (size_t)r1 * rowb, min(nr, nrow_all - r1) * rowb,
+                          lane);
+          copy_async_wait<1>();
+        } else {
+          copy_async_wait<0>();
         }
-      }
-      if (!MIXED) {
-        // whole Chebyshev slabs per chunk, AoS double2 per proxy
-        constexpr int W = DL ? 6 : 3;
-        const int S2 = P1 * P1;
-        const int nsl = max(1, (kSmem / (2 * W)) / S2);
-        for (int sl0 = 0; sl0 < P1; sl0 += nsl) {
-          const int ns = min(nsl, P1 - sl0);
-          const int kk0 = sl0 * S2, cnt = ns * S2;
-          __syncthreads();
-          for (int e = tid; e < cnt * C; e += kTB) {
-            const int c = e / cnt, q = e - c * cnt;
-            sm[q * 2 * W + c] = M[(size_t)c * Pf + kk0 + q];
-          }
-          __syncthreads();
-          if (wm != 0u && act) {
-            proxies64_slabs<DL>(reinterpret_cast<const double2*>(sm), ns, sl0, P1, cheb, S, a0, a1, a2);
-            if (kCount) cprox += cnt;
-          }
+        __syncwarp();
+        if (act) {
+          const char* cur = buf + (ch & 1) * kHalf;
+          if (MIXED)
+            proxies32_rows<DL>(reinterpret_cast<const float4*>(cur), row0, rows, P1, wchebf, F, a0, a1, a2);
+          else
+            proxies64_rows<DL>(reinterpret_cast<const double2*>(cur), row0, rows, P1, wcheb, S, a0, a1, a2);
         }
+        __syncwarp();
       }
+      if (kCount && act) cprox += Pf;
     }
   }
   // partial sums of this item
@@ -834,11 +845,10 @@ __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict
                                                       const BlockRef* __restrict__ items,
                                                       const Seg* __restrict__ segs) {
   __shared__ __align__(16) double sm[kSmem];
-  // FP32 source tile: (x, y, z, area), (n, 0), (q, 0) per source; also holds
-  // the FP32 proxy moments of whole Chebyshev slabs (3 or 2 float4 per proxy)
-  __shared__ float4 sf[MIXED ? 3 * kNT : 1];
-  __shared__ double cheb[3 * kMaxP1];
-  __shared__ float chebf[3 * kMaxP1];
+  // per-warp FP32 source tiles: (x, y, z, area), (n, 0), (q, 0) per source
+  __shared__ float4 sf[MIXED ? kWarps * 3 * kNT : 1];
+  __shared__ double cheb[kWarps * 3 * kMaxP1];
+  __shared__ float chebf[kWarps * 3 * kMaxP1];
   __shared__ EvalTask sT;
   // smoothing tables: G1, G2 for the Stokeslet family, G3 for the stresslet family
   __shared__ double stab[FAM == F_SL ? 2 * kSmoothN : (FAM == F_DL ? kSmoothN : 1)];

@@ -91,6 +91,8 @@ void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direc
   partial.alloc((size_t)std::max(1, nitems) * 12 * Pf);
   mom.alloc((size_t)nn * 12 * Pf);
   mom.zero(st);
+  momf.alloc((size_t)nn * 12 * Pf);
+  momf.zero(st);
 }
 
 void Ctx::check_tc() {
@@ -114,12 +116,12 @@ void DevTree::set_density(Ctx& C, const double* q3_dev, bool dl, bool moments, b
     }
     launch_moments_tc(dl ? 1 : 0, items.p, nitems, P1, tcheb.p, x.p, y.p, z.p, nx.p, ny.p, nz.p, a.p, qx.p, qy.p,
                       qz.p, partial.p, C.tc_err.p, C.stream);
-    launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, C.stream);
+    launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, momf.p, C.stream);
     C.launches += 2;
   } else if (moments && nitems > 0) {
     launch_moments(dl ? 1 : 0, items.p, nitems, P1, tcheb.p, x.p, y.p, z.p, nx.p, ny.p, nz.p, a.p,
                    qx.p, qy.p, qz.p, partial.p, C.stream);
-    launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, C.stream);
+    launch_moments_reduce(dl ? 12 : 6, Pf, nn, item_start.p, partial.p, mom.p, momf.p, C.stream);
     C.launches += 2;
   }
 }
@@ -177,6 +179,7 @@ EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const D
   k.node_m1 = T.m1.p;
   k.tcheb = T.tcheb.p;
   k.mom = T.mom.p;
+  k.momf = T.momf.p;
   k.tord = L.tord.p;
   k.txyz = tg.xyz.p;
   k.tb = tg.b.p;
@@ -197,7 +200,7 @@ EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const D
 void Batch::finalize(cudaStream_t st, int num_sms) {
   // 1. segments: a far entry whole, a near entry cut into source ranges of
   //    at most kSegSrc; cost ~ active warps x pair evaluations.
-  constexpr int kSegSrc = 1024;
+  constexpr int kSegSrc = 512;
   struct HSeg {
     Seg s;
     double cost;
@@ -231,8 +234,9 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
     }
   }
   // 2. items: runs of consecutive segments of one block, each about
-  //    total / (SMs x 4 resident CTAs x 6 waves), never below four tiles.
-  const double target = std::max(total / (num_sms * 4.0 * 6.0), 4.0 * 256.0 * 2.0);
+  //    total / (SMs x 4 resident CTAs x 16 waves), never below two tiles;
+  //    small items keep the tail short where the cost estimate is off.
+  const double target = std::max(total / (num_sms * 4.0 * 16.0), 2.0 * 256.0 * 2.0);
   std::vector<Seg> segs;
   std::vector<std::pair<double, BlockRef>> items;
   std::vector<int> starts;

@@ -473,8 +473,15 @@ class Plan2S:
         self.ctx._check(lib().hr_plan2s_check_upward_pass(self.p, _dp(_f64(x)), ctypes.byref(v)))
         return v.value
 
+    def set_inner_tree(self, P, N0, theta=0.6):
+        """Own treecode (degree P, leaf size N0, MAC theta) for the reduced-precision
+        inner operator of GMRES-IR; P = 0 removes it. FP64 true residuals keep the
+        plan's treecode."""
+        self.ctx._check(lib().hr_plan2s_set_inner_tree(self.p, int(P), int(N0), ctypes.c_double(theta)))
+
     def time_batch(self, which=0, iters=10):
-        """Milliseconds per launch of one boundary-sum batch (0 DL fp64, 1 SL, 2 DL mixed)."""
+        """Milliseconds per launch of one boundary-sum batch (0 DL fp64, 1 SL, 2 DL mixed,
+        3 DL mixed on the inner treecode)."""
         v = ctypes.c_double()
         self.ctx._check(lib().hr_plan2s_time_batch(self.p, which, iters, ctypes.byref(v)))
         return v.value

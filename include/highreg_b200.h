@@ -211,7 +211,10 @@ typedef struct {
    * b - A x starts the next cycle; the solve ends when that FP64 residual
    * meets tol. mixed_accuracy: relative accuracy of a reduced-precision
    * matvec (0 = 3e-7 for HR_MIXED, whose measured max-norm relative error
-   * is 2.7e-7, and 1e-6 for HR_FP32). */
+   * is 2.7e-7, and 1e-6 for HR_FP32; with an inner treecode,
+   * hr_plan2s_set_inner_tree, the inner operator's accuracy). With
+   * use_guess, the guess's first residual comes from the reduced-precision
+   * operator, and a guess that already meets tol is confirmed in FP64. */
   double mixed_accuracy;
 } hr_gmres_opts;
 
@@ -260,12 +263,21 @@ int hr_plan2s_work(hr_plan2s* plan, int which /*0 matvec, 1 rhs*/, hr_work* w);
  * the FP64 ones; max over nodes and channels of max |difference| / max |FP64
  * moment|. HR_TREE plans only. */
 int hr_plan2s_check_upward_pass(hr_plan2s* plan, const double* x, double* max_rel_err);
+/* Gives the reduced-precision inner operator of GMRES-IR (HR_MIXED and
+ * HR_FP32 solves) a treecode of its own: KITC with degree P, leaf size N0 and
+ * MAC theta over the same surfaces, targets and density stencils. The inner
+ * Krylov cycles then apply this cheaper operator, while every FP64 true
+ * residual, and with it the stopping test, still applies the plan's own
+ * treecode: the converged answer meets the same residual tolerance. P = 0
+ * removes it. HR_TREE plans only. */
+int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double theta);
 /* the plan's stream (cudaStream_t) for callers that enqueue their own work */
 void* hr_plan2s_stream(hr_plan2s* plan);
 /* Times `iters` back-to-back launches of one boundary-sum batch with CUDA
  * events on the plan's stream (inputs as left by the last matvec / RHS):
  * which 0 = stresslet batch (matvec, FP64), 1 = Stokeslet batch (RHS),
- * 2 = stresslet batch (mixed precision). Returns milliseconds per launch. */
+ * 2 = stresslet batch (mixed precision), 3 = the inner treecode's mixed
+ * stresslet batch. Returns milliseconds per launch. */
 int hr_plan2s_time_batch(hr_plan2s* plan, int which, int iters, double* ms_per_launch);
 
 /* ------------------------------------------- two-surface geometry setup */

@@ -96,6 +96,37 @@ def test_fp32_solve_reaches_fp64_residual(plan32, geo32):
     assert rel_err(x32, x64) < 1e-8
 
 
+def test_inner_tree_solve_reaches_fp64_residual(ctx, geo32):
+    """GMRES-IR whose inner cycles run on a coarser treecode (P = 4, N0 = 300):
+    the FP64 true residual, taken with the plan's own treecode, still meets the
+    tolerance, and the solution matches the all-FP64 one to 1e-8."""
+    p = highreg.Plan2S(ctx, geo32, mode=highreg.HR_TREE, P=6, N0=1000, theta=0.6)
+    b = p.rhs(geo32["f0"], geo32["f1"])
+    x64, r64 = p.solve(b, restart=50, tol=1e-10, true_residual=True)
+    u = np.random.default_rng(5).standard_normal(p.n)
+    ym = torch.zeros(p.n, dtype=torch.float64, device="cuda")
+    yi = torch.zeros_like(ym)
+    ut = torch.tensor(u, dtype=torch.float64, device="cuda")
+    p.matvec_dev(ut, ym, highreg.HR_MIXED)
+    p.set_inner_tree(4, 300, 0.6)
+    p.matvec_dev(ut, yi, highreg.HR_MIXED)
+    torch.cuda.synchronize()
+    e_inner = rel_err(yi.cpu().numpy(), ym.cpu().numpy())
+    print("inner-treecode operator vs the plan's (mixed):", e_inner)
+    assert 0 < e_inner < 1e-2  # P = 4 against P = 6: ~2e-3 at h = 1/32
+    xi, ri = p.solve(b, restart=50, tol=1e-10, precision=highreg.HR_MIXED, mixed_accuracy=max(e_inner, 3e-7))
+    print("inner-treecode solve:", ri["iterations"], "iterations,", ri["matvecs_fp64"], "FP64 matvecs")
+    assert ri["matvecs_mixed"] > 0
+    assert ri["true_residual"] <= 1e-10
+    assert rel_err(xi, x64) < 1e-8
+    # removing it restores the plan's own operator
+    p.set_inner_tree(0, 0)
+    p.matvec_dev(ut, yi, highreg.HR_MIXED)
+    torch.cuda.synchronize()
+    assert rel_err(yi.cpu().numpy(), ym.cpu().numpy()) == 0.0
+    p.close()
+
+
 @pytest.mark.parametrize("P,N0", [(6, 1000), (10, 2000), (4, 300)])
 def test_tensor_core_upward_pass_matches_fp64(ctx, geo32, P, N0):
     """The 3xTF32 tcgen05 upward pass (reduced-precision operator) against the
