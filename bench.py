@@ -320,13 +320,13 @@ def run_ours(args, rank, world, local_rank):
     # and leaf size); the FP64 true residuals keep the benchmark's treecode
     ms_dl_inner = None
     if INNER is not None:
-        plan.set_inner_tree(INNER[0], INNER[1], THETA)
+        inner_err = plan.set_inner_tree(INNER[0], INNER[1], THETA)
         for name, g in (("mixed_inner", None), ("mixed_inner_warm", guess)):
             if name.endswith("warm") and g is None:
                 continue
             timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, g)
             v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, args.steps, g)
-            v["inner_tree"] = {"P": INNER[0], "N0": INNER[1], "theta": THETA}
+            v["inner_tree"] = {"P": INNER[0], "N0": INNER[1], "theta": THETA, "rel_l2_error": inner_err}
             variants[name] = v
         plan.matvec_dev(x, b, highreg.HR_MIXED)
         ms_dl_inner = plan.time_batch(3, 20)
@@ -363,7 +363,7 @@ def run_ours(args, rank, world, local_rank):
         # dram__bytes_read.sum + dram__bytes_write.sum of this launch from one ncu capture
         # (profiles/eval_kernel_fp64_stresslet_h64.md): sources are staged once per tile, so
         # DRAM traffic is tiny next to the compute; the bound is the FP64 pipe
-        roofline["traffic"] = 16364032 + 1024
+        roofline["traffic"] = 16167680 + 1762304
         roofline["traffic_source"] = "ncu capture of this kernel at this workload"
 
     # end to end through the C ABI with host buffers: scene upload + plan
@@ -527,13 +527,13 @@ def main():
                     help="2s: the two-surface solve (the benchmark); e2g: the extend-to-grid pipeline")
     ap.add_argument("--N", type=int, default=96, help="extend-to-grid grid size (96 or 384)")
     ap.add_argument("--inner", default="auto",
-                    help="treecode 'P,N0' of the mixed solve's inner operator; 'auto': 6,2000 when the "
-                         "workload's treecode is finer, 'none': no inner treecode")
+                    help="treecode 'P,N0' of the mixed solve's inner operator; 'auto': 5,2000 when the "
+                         "workload's P is above 6, 'none': no inner treecode")
     args = ap.parse_args()
     global H_INV, P, N0, INNER
     H_INV, P, N0 = args.h, args.P, args.N0
     if args.inner == "auto":
-        INNER = (6, 2000) if (P, N0) != (6, 2000) and P >= 6 else None
+        INNER = (5, 2000) if P > 6 else None
     elif args.inner == "none":
         INNER = None
     else:

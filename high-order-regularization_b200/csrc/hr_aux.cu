@@ -103,27 +103,42 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(
 }
 
 // Sums the partial moments of each node in item order (deterministic) and
-// stores them proxy-major: FP64 C doubles per proxy, and an FP32 copy with W32
-// floats per proxy (12 for the stresslet's 12 channels, 8 for the Stokeslet's
-// 6 plus two zeros), so that a warp reads one proxy's moments as a few
-// contiguous vector loads.
+// stores them proxy-major, one thread per proxy. The stresslet's 12 channels
+// (g (x) n, g-major, then n) enter the far field only through
+//   d.M.d = M00 d0^2 + M11 d1^2 + M22 d2^2 + (M01 + M10) d0 d1
+//         + (M02 + M20) d0 d2 + (M12 + M21) d1 d2   and   Mn.d,
+// so they are stored as those 6 symmetric combinations and Mn: FP64 10
+// doubles per proxy (the last one zero), FP32 12 floats (the last three zero).
+// The Stokeslet's 6 channels (f, n) are stored as they are: FP64 6 doubles,
+// FP32 8 floats (the last two zero).
 __global__ void moments_reduce_kernel(int C, int Pf, const int* __restrict__ item_start,
                                       const double* __restrict__ partial, double* __restrict__ mom,
                                       float* __restrict__ momf) {
   const int node = blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int CP = C * Pf;
-  if (i >= CP) return;
-  const int c = i / Pf, kk = i - c * Pf;
-  const int W32 = C == 12 ? 12 : 8;
+  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+  if (kk >= Pf) return;
   const int a = item_start[node], b = item_start[node + 1];
-  double s = 0.0;
-  for (int q = a; q < b; q++) s += partial[(size_t)q * CP + i];
-  s = (a < b) ? s : 0.0;
-  mom[((size_t)node * Pf + kk) * C + c] = s;
-  float* f = momf + ((size_t)node * Pf + kk) * W32;
-  f[c] = (float)s;
-  if (C == 6 && c < 2) f[6 + c] = 0.f;
+  double m[12];
+#pragma unroll
+  for (int c = 0; c < 12; c++) m[c] = 0.0;
+  for (int q = a; q < b; q++) {
+#pragma unroll
+    for (int c = 0; c < 12; c++)
+      if (c < C) m[c] += partial[((size_t)q * C + c) * Pf + kk];
+  }
+  const size_t k = (size_t)node * Pf + kk;
+  if (C == 12) {
+    const double o[10] = {m[0], m[4], m[8], m[1] + m[3], m[2] + m[6], m[5] + m[7], m[9], m[10], m[11], 0.0};
+#pragma unroll
+    for (int i = 0; i < 10; i++) mom[k * 10 + i] = o[i];
+#pragma unroll
+    for (int i = 0; i < 12; i++) momf[k * 12 + i] = i < 9 ? (float)o[i] : 0.f;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 6; i++) mom[k * 6 + i] = m[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) momf[k * 8 + i] = i < 6 ? (float)m[i] : 0.f;
+  }
 }
 
 __global__ void permute_kernel(int n, const int* __restrict__ perm, const double* __restrict__ q3,
@@ -326,8 +341,8 @@ void launch_moments(int dl, const MomItem* d_items, int nitems, int P1, const do
 void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_start,
                            const double* partial, double* mom, float* momf, cudaStream_t st) {
   if (nnodes_out <= 0) return;
-  dim3 grid((C * Pf + 255) / 256, nnodes_out);
-  moments_reduce_kernel<<<grid, 256, 0, st>>>(C, Pf, d_item_start, partial, mom, momf);
+  dim3 grid((Pf + 127) / 128, nnodes_out);
+  moments_reduce_kernel<<<grid, 128, 0, st>>>(C, Pf, d_item_start, partial, mom, momf);
 }
 
 void launch_permute(int n, const int* perm, const double* q3, double* qx, double* qy, double* qz,

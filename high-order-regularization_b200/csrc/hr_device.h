@@ -14,7 +14,7 @@ struct EvalTask {
   int kind;       // Kind
   int jump_mode;  // DL kinds: 0 = treecode convention, 1 = direct-sum convention
   int P1, Pf;     // treecode degree + 1 and (P+1)^3
-  int C;          // moment channels stored per node (6 SL, 12 DL)
+  int C;          // FP64 moment values stored per proxy (6 SL, 10 DL)
   int nt;         // number of targets
   int mixed;      // 0 FP64; 1: pairs beyond 3 delta and proxies in FP32 (FP64 accumulation); 2: all pairs FP32
   int pad;

@@ -544,36 +544,37 @@ __device__ __forceinline__ void copy_async_wait() {
 
 // Proxy interactions of a run of Chebyshev rows (row r = i (P+1) + j holds
 // proxies (i, j, 0..P)) from the warp's shared copy of the node's proxy-major
-// moments: FP64 as double2 (DL 6, SL 3 per proxy), FP32 as float4 (DL: M00
-// M01 M02 M10 | M11 M12 M20 M21 | M22 Mn0 Mn1 Mn2; SL: f0 f1 f2 n0 | n1 n2 - -).
-// Every lane reads the same proxy (a shared-memory broadcast). The stresslet
-// kernel uses
+// moments: FP64 as double2 (DL 5, SL 3 per proxy), FP32 as float4 (DL 3, SL 2).
+// Stresslet per proxy: S = (M00, M11, M22, M01 + M10, M02 + M20, M12 + M21),
+// Mn (and padding); Stokeslet: f, n. Every lane reads the same proxy (a
+// shared-memory broadcast). The stresslet kernel uses
 //   sum_l (sum_k (M[3l+k] - g0_l Mn_k) d_k) d_l = d.M.d - (g0.d)(Mn.d),
 // the reference's proxy sum (Call_Treecode_DL, 2S/KITC.cpp:753-771)
-// regrouped; Call_Treecode_SL (2S/KITC.cpp:700-714) as written.
+// regrouped, with d.M.d from the symmetric part and the products of d0, d1
+// taken once per row; Call_Treecode_SL (2S/KITC.cpp:700-714) as written.
 template <bool DL>
 __device__ __forceinline__ void proxies64_rows(const double2* __restrict__ s2, int row0, int nrows, int P1,
                                                const double* __restrict__ cheb, const Tgt& S, double& a0,
                                                double& a1, double& a2) {
-  constexpr int W = DL ? 6 : 3;  // double2 per proxy
+  constexpr int W = DL ? 5 : 3;  // double2 per proxy
   for (int r = 0; r < nrows; r++) {
     const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
     const double d0 = S.px - cheb[pi];
     const double d1 = S.py - cheb[P1 + pj];
     const double r01 = d0 * d0 + d1 * d1;
+    const double d00 = d0 * d0, d11 = d1 * d1, d01 = d0 * d1;
+    const double g0r = S.g0[0] * d0 + S.g0[1] * d1;
     const double2* row = s2 + r * P1 * W;
     for (int pk = 0; pk < P1; pk++) {
       const double d2 = S.pz - cheb[2 * P1 + pk];
       const double rinv = rsqrt(fma(d2, d2, r01));
       const double2* m = row + pk * W;
       if (DL) {
-        const double2 m01 = m[0], m23 = m[1], m45 = m[2], m67 = m[3], m89 = m[4], m1011 = m[5];
-        const double u0 = m01.x * d0 + m01.y * d1 + m23.x * d2;
-        const double u1 = m23.y * d0 + m45.x * d1 + m45.y * d2;
-        const double u2 = m67.x * d0 + m67.y * d1 + m89.x * d2;
-        const double dmd = d0 * u0 + d1 * u1 + d2 * u2;
-        const double mnd = m89.y * d0 + m1011.x * d1 + m1011.y * d2;
-        const double g0d = S.g0[0] * d0 + S.g0[1] * d1 + S.g0[2] * d2;
+        const double2 s01 = m[0], s23 = m[1], s45 = m[2], n01 = m[3], n2 = m[4];
+        const double dmd = s01.x * d00 + s01.y * d11 + s23.x * (d2 * d2) + s23.y * d01 + s45.x * (d0 * d2) +
+                           s45.y * (d1 * d2);
+        const double mnd = n01.x * d0 + n01.y * d1 + n2.x * d2;
+        const double g0d = fma(S.g0[2], d2, g0r);
         const double ri2 = rinv * rinv;
         const double kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
         a0 += d0 * kernel;
@@ -604,6 +605,8 @@ __device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, in
     const float d0 = F.px - chebf[pi];
     const float d1 = F.py - chebf[P1 + pj];
     const float r01 = d0 * d0 + d1 * d1;
+    const float d00 = d0 * d0, d11 = d1 * d1, d01 = d0 * d1;
+    const float g0r = F.g0[0] * d0 + F.g0[1] * d1;
     const float4* row = s4 + r * P1 * W;
     float p0 = 0.f, p1 = 0.f, p2 = 0.f;
     for (int pk = 0; pk < P1; pk++) {
@@ -612,13 +615,10 @@ __device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, in
       const float4 A = row[pk * W];
       const float4 B = row[pk * W + 1];
       if (DL) {
-        const float4 Cc = row[pk * W + 2];
-        const float u0 = A.x * d0 + A.y * d1 + A.z * d2;
-        const float u1 = A.w * d0 + B.x * d1 + B.y * d2;
-        const float u2 = B.z * d0 + B.w * d1 + Cc.x * d2;
-        const float dmd = d0 * u0 + d1 * u1 + d2 * u2;
-        const float mnd = Cc.y * d0 + Cc.z * d1 + Cc.w * d2;
-        const float g0d = F.g0[0] * d0 + F.g0[1] * d1 + F.g0[2] * d2;
+        const float Cx = reinterpret_cast<const float*>(row + pk * W + 2)[0];
+        const float dmd = A.x * d00 + A.y * d11 + A.z * (d2 * d2) + A.w * d01 + B.x * (d0 * d2) + B.y * (d1 * d2);
+        const float mnd = B.z * d0 + B.w * d1 + Cx * d2;
+        const float g0d = fmaf(F.g0[2], d2, g0r);
         const float ri2 = rinv * rinv;
         const float kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
         p0 += d0 * kernel;
@@ -779,7 +779,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
       // The node's proxy-major moments stream through the warp's tile in
       // runs of whole Chebyshev rows, double-buffered: the asynchronous copy
       // of the next run overlaps the interactions of this one.
-      constexpr int kBpp = MIXED ? (DL ? 48 : 32) : (DL ? 96 : 48);  // bytes per proxy
+      constexpr int kBpp = MIXED ? (DL ? 48 : 32) : (DL ? 80 : 48);  // bytes per proxy
       constexpr int kHalf = kWarpSm * 4;                              // bytes per buffer
       const char* src = MIXED ? reinterpret_cast<const char*>(T.momf + (size_t)E.node * Pf * (DL ? 12 : 8))
                               : reinterpret_cast<const char*>(T.mom + (size_t)E.node * Pf * C);

@@ -149,7 +149,7 @@ EvalTask make_task(int kind, double DEL, double scale, const DevTree& T, const D
   k.jump_mode = 0;
   k.P1 = T.P1;
   k.Pf = T.Pf;
-  k.C = (kind == K_DL_ON || kind == K_DL_OFF) ? 12 : 6;
+  k.C = (kind == K_DL_ON || kind == K_DL_OFF) ? 10 : 6;
   k.nt = tg.n;
   k.mixed = 0;
   k.DEL = DEL;

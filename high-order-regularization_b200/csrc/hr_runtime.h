@@ -97,7 +97,7 @@ struct DevTree {
   DBuf<double> qx, qy, qz;
   DBuf<float> fx, fy, fz, fnx, fny, fnz, fa, fqx, fqy, fqz;  // FP32 copies, centre-relative
   double ctr[3] = {0, 0, 0};
-  DBuf<double> mom;  // nn * Pf * C, proxy-major (C = 12 DL, 6 SL)
+  DBuf<double> mom;  // nn * Pf * C, proxy-major (C = 10 DL symmetric form, 6 SL)
   DBuf<float> momf;  // nn * Pf * W32 FP32 copy (W32 = 12 DL, 8 SL)
   DBuf<MomItem> items;
   DBuf<int> item_start;

@@ -476,8 +476,12 @@ class Plan2S:
     def set_inner_tree(self, P, N0, theta=0.6):
         """Own treecode (degree P, leaf size N0, MAC theta) for the reduced-precision
         inner operator of GMRES-IR; P = 0 removes it. FP64 true residuals keep the
-        plan's treecode."""
-        self.ctx._check(lib().hr_plan2s_set_inner_tree(self.p, int(P), int(N0), ctypes.c_double(theta)))
+        plan's treecode. Returns the inner operator's measured relative L2 error
+        (0 when removed), the default mixed_accuracy of later solves."""
+        e = ctypes.c_double(0.0)
+        self.ctx._check(lib().hr_plan2s_set_inner_tree(self.p, int(P), int(N0), ctypes.c_double(theta),
+                                                       ctypes.byref(e)))
+        return e.value
 
     def time_batch(self, which=0, iters=10):
         """Milliseconds per launch of one boundary-sum batch (0 DL fp64, 1 SL, 2 DL mixed,

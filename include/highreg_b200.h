@@ -212,7 +212,7 @@ typedef struct {
    * meets tol. mixed_accuracy: relative accuracy of a reduced-precision
    * matvec (0 = 3e-7 for HR_MIXED, whose measured max-norm relative error
    * is 2.7e-7, and 1e-6 for HR_FP32; with an inner treecode,
-   * hr_plan2s_set_inner_tree, the inner operator's accuracy). With
+   * hr_plan2s_set_inner_tree, at least its measured accuracy). With
    * use_guess, the guess's first residual comes from the reduced-precision
    * operator, and a guess that already meets tol is confirmed in FP64. */
   double mixed_accuracy;
@@ -268,9 +268,12 @@ int hr_plan2s_check_upward_pass(hr_plan2s* plan, const double* x, double* max_re
  * MAC theta over the same surfaces, targets and density stencils. The inner
  * Krylov cycles then apply this cheaper operator, while every FP64 true
  * residual, and with it the stopping test, still applies the plan's own
- * treecode: the converged answer meets the same residual tolerance. P = 0
- * removes it. HR_TREE plans only. */
-int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double theta);
+ * treecode: the converged answer meets the same residual tolerance. The
+ * inner operator's relative L2 error against the plan's FP64 one, on a fixed
+ * pseudo-random density, is measured here (written to *rel_err if not NULL)
+ * and is the default mixed_accuracy of later solves. P = 0 removes it.
+ * HR_TREE plans only. */
+int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double theta, double* rel_err);
 /* the plan's stream (cudaStream_t) for callers that enqueue their own work */
 void* hr_plan2s_stream(hr_plan2s* plan);
 /* Times `iters` back-to-back launches of one boundary-sum batch with CUDA
