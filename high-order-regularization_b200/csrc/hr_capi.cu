@@ -60,6 +60,16 @@ void check_finite(const double* a, size_t n, const char* what) {
     if (!std::isfinite(a[i])) throw hr::Error(HR_ERR_NAN, std::string("non-finite value in ") + what);
 }
 
+// Monge-patch axes (ind1, ind2, ind3) of every interpolating target must be
+// coordinate indices 0..2.
+void check_i123(int n, const int* nrst, const int* i123) {
+  for (int i = 0; i < n; i++)
+    if (nrst[i] != 0)
+      for (int k = 0; k < 3; k++)
+        if (i123[3 * i + k] < 0 || i123[3 * i + k] > 2)
+          throw hr::Error(HR_ERR_ARG, "i123 entries must be 0, 1 or 2");
+}
+
 // near = the regularized branch: |b| / delta <= 8 (2S/KITC.cpp:856, 970; 2S/stokeslets.cpp:40)
 std::vector<uint8_t> near_flags(int n, const double* b, double delta) {
   std::vector<uint8_t> v(n, 1);
@@ -339,6 +349,7 @@ extern "C" int hr_interpolate_dl_density(hr_ctx* ctx, double h, const hr_surface
     HR_REQUIRE(S->n == 0 || (S->xyz && g), "surface arrays missing");
     HR_CHECK_CUDA(cudaSetDevice(ctx->c.device));
     cudaStream_t st = ctx->c.stream;
+    check_i123(T->n, T->nrst, T->i123);
     Stencils s = build_stencils(h, S->center, S->n, S->xyz, T->n, T->nrst, T->x0, T->i123);
     if (S->n == 0) {
       for (size_t e = 0; e < s.tgt.size(); e++) HR_REQUIRE(false, "interpolation from an empty surface");
@@ -803,6 +814,7 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
       P->Lon[t].build(P->tree[t].host, T.n, sc->surf[t].xyz, all.data(), st);
       P->Loff[t].build(P->tree[1 - t].host, T.n, sc->surf[t].xyz, near.data(), st);
       const hr_surface& Ssrc = sc->surf[1 - t];
+      check_i123(T.n, T.nrst, T.i123);
       Stencils s = build_stencils(sc->h, Ssrc.center, Ssrc.n, Ssrc.xyz, T.n, T.nrst, T.x0, T.i123);
       P->sten[t].build(s, st);
       P->out_on[t].alloc(3 * (size_t)T.n);

@@ -196,7 +196,8 @@ std::vector<int> morton_order(int n, const double* xyz) {
     v = (v | v << 2) & 0x1249249249249249ULL;
     return v;
   };
-  std::vector<uint64_t> code(n);
+  std::vector<uint64_t> code(n), code2(n);
+#pragma omp parallel for schedule(static)
   for (int i = 0; i < n; i++) {
     uint64_t q[3];
     for (int k = 0; k < 3; k++) {
@@ -206,7 +207,21 @@ std::vector<int> morton_order(int n, const double* xyz) {
     }
     code[i] = spread(q[0]) | (spread(q[1]) << 1) | (spread(q[2]) << 2);
   }
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return code[a] < code[b]; });
+  // stable LSD radix sort of the 63-bit codes, 11 bits per pass
+  std::vector<int> ord2(n);
+  for (int shift = 0; shift < 63; shift += 11) {
+    int cnt[2049] = {0};
+    for (int i = 0; i < n; i++) cnt[((code[i] >> shift) & 2047) + 1]++;
+    for (int d = 0; d < 2048; d++) cnt[d + 1] += cnt[d];
+    for (int i = 0; i < n; i++) {
+      const int d = (int)((code[i] >> shift) & 2047);
+      const int p = cnt[d]++;
+      code2[p] = code[i];
+      ord2[p] = ord[i];
+    }
+    code.swap(code2);
+    ord.swap(ord2);
+  }
   return ord;
 }
 
@@ -303,34 +318,72 @@ Stencils build_stencils(double h, const double ctr[3], int nq, const double* xq,
                         const int* nrst, const double* x0, const int* i123) {
   Stencils S;
   // Grid-line candidates per orientation ind3 (the interpolation plane is
-  // spanned by the two other axes, ind1 < ind2): key (kx, ky, side).
-  struct Key {
-    long long v;
-    bool operator==(const Key& o) const { return v == o.v; }
-  };
-  struct KeyHash {
-    size_t operator()(const Key& k) const { return std::hash<long long>()(k.v); }
-  };
-  auto mk = [](long long kx, long long ky, int side) {
-    return Key{((kx + (1LL << 30)) << 32) ^ ((ky + (1LL << 30)) << 1) ^ (long long)side};
-  };
+  // spanned by the two other axes, ind1 < ind2): quadrature points lying on
+  // grid line (kx, ky) of that plane, on side z > 0 or z < 0, in a dense
+  // (kx, ky, side) cell table in CSR form, ascending point index per cell.
   const int i1s[3] = {1, 0, 0}, i2s[3] = {2, 2, 1};  // by ind3 = 0, 1, 2
-  std::unordered_map<Key, std::vector<int>, KeyHash> maps[3];
-  for (int o = 0; o < 3; o++) {
-    int a1 = i1s[o], a2 = i2s[o];
-    for (int j = 0; j < nq; j++) {
-      double X = xq[3 * j + a1], Y = xq[3 * j + a2];
-      double z = xq[3 * j + o] - ctr[o];
-      if (!(z > 0) && !(z < 0)) continue;
-      long long kx = llround((X - ctr[a1]) / h), ky = llround((Y - ctr[a2]) / h);
-      if (fabs(X - (kx * h + ctr[a1])) > 1e-11 || fabs(Y - (ky * h + ctr[a2])) > 1e-11) continue;
-      maps[o][mk(kx, ky, z > 0 ? 1 : 0)].push_back(j);
+  struct Grid {
+    long long kx0 = 0, ky0 = 0;
+    long long nx = 0, ny = 0;
+    std::vector<int> start, items;
+    int cell(long long kx, long long ky, int side) const {
+      if (kx < kx0 || ky < ky0 || kx >= kx0 + nx || ky >= ky0 + ny) return -1;
+      return (int)((((kx - kx0) * ny) + (ky - ky0)) * 2 + side);
     }
+  } G[3];
+  for (int o = 0; o < 3; o++) {
+    const int a1 = i1s[o], a2 = i2s[o];
+    std::vector<long long> key(2 * (size_t)nq);
+    std::vector<int> side(nq, -1);
+    long long kxmin = 0, kxmax = -1, kymin = 0, kymax = -1;
+    for (int j = 0; j < nq; j++) {
+      const double X = xq[3 * j + a1], Y = xq[3 * j + a2];
+      const double z = xq[3 * j + o] - ctr[o];
+      if (!(z > 0) && !(z < 0)) continue;
+      const long long kx = llround((X - ctr[a1]) / h), ky = llround((Y - ctr[a2]) / h);
+      if (fabs(X - (kx * h + ctr[a1])) > 1e-11 || fabs(Y - (ky * h + ctr[a2])) > 1e-11) continue;
+      key[2 * j] = kx;
+      key[2 * j + 1] = ky;
+      side[j] = z > 0 ? 1 : 0;
+      if (kxmax < kxmin) {
+        kxmin = kxmax = kx;
+        kymin = kymax = ky;
+      } else {
+        kxmin = std::min(kxmin, kx);
+        kxmax = std::max(kxmax, kx);
+        kymin = std::min(kymin, ky);
+        kymax = std::max(kymax, ky);
+      }
+    }
+    Grid& g = G[o];
+    g.kx0 = kxmin;
+    g.ky0 = kymin;
+    g.nx = kxmax - kxmin + 1;
+    g.ny = kymax - kymin + 1;
+    const size_t ncell = (size_t)std::max(0LL, g.nx * g.ny * 2);
+    g.start.assign(ncell + 1, 0);
+    for (int j = 0; j < nq; j++)
+      if (side[j] >= 0) g.start[g.cell(key[2 * j], key[2 * j + 1], side[j]) + 1]++;
+    for (size_t c = 0; c < ncell; c++) g.start[c + 1] += g.start[c];
+    g.items.resize(g.start[ncell]);
+    std::vector<int> fill(g.start.begin(), g.start.end() - 1);
+    for (int j = 0; j < nq; j++)
+      if (side[j] >= 0) g.items[fill[g.cell(key[2 * j], key[2 * j + 1], side[j])]++] = j;
   }
+  std::vector<int> ent(nt, -1);
+  int ne = 0;
+  for (int i = 0; i < nt; i++)
+    if (nrst[i] != 0) ent[i] = ne++;
+  S.tgt.resize(ne);
+  S.idx.assign(36 * (size_t)ne, 0);
+  S.pq.resize(2 * (size_t)ne);
+#pragma omp parallel for schedule(dynamic, 256)
   for (int i = 0; i < nt; i++) {
-    if (nrst[i] == 0) continue;
+    const int e = ent[i];
+    if (e < 0) continue;
     const double* X0 = &x0[3 * i];
-    int ind1 = i123[3 * i], ind2 = i123[3 * i + 1], ind3 = i123[3 * i + 2];
+    const int ind1 = i123[3 * i], ind2 = i123[3 * i + 1], ind3 = i123[3 * i + 2];
+    const bool ok_plane = (ind3 >= 0 && ind3 < 3) && (ind1 == i1s[ind3] && ind2 == i2s[ind3]);
     double xLow = floor((X0[ind1] - ctr[ind1]) / h) * h + ctr[ind1];
     double yLow = floor((X0[ind2] - ctr[ind2]) / h) * h + ctr[ind2];
     double xHigh = xLow + h, yHigh = yLow + h;
@@ -338,25 +391,24 @@ Stencils build_stencils(double h, const double ctr[3], int nq, const double* xq,
     const double tol = 1.e-14;
     double cx[6] = {xLow - 2.0 * h, xLow - h, xLow, xHigh, xHigh + h, xHigh + 2.0 * h};
     double cy[6] = {yLow - 2.0 * h, yLow - h, yLow, yHigh, yHigh + h, yHigh + 2.0 * h};
-    int st[36];
-    for (int q = 0; q < 36; q++) st[q] = 0;
-    bool ok_plane = (ind3 >= 0 && ind3 < 3) && (ind1 == i1s[ind3] && ind2 == i2s[ind3]);
+    int* st = &S.idx[36 * (size_t)e];
     if (ok_plane && (z0 > 0 || z0 < 0)) {
-      const auto& M = maps[ind3];
-      int side = z0 > 0 ? 1 : 0;
+      const Grid& g = G[ind3];
+      const int side = z0 > 0 ? 1 : 0;
       for (int a = 0; a < 6; a++)
         for (int bq = 0; bq < 6; bq++) {
-          long long kx = llround((cx[a] - ctr[ind1]) / h), ky = llround((cy[bq] - ctr[ind2]) / h);
-          auto it = M.find(mk(kx, ky, side));
-          if (it == M.end()) continue;
+          const long long kx = llround((cx[a] - ctr[ind1]) / h), ky = llround((cy[bq] - ctr[ind2]) / h);
+          const int c = g.cell(kx, ky, side);
+          if (c < 0) continue;
           int best = -1;
-          for (int j : it->second) {
+          for (int q = g.start[c]; q < g.start[c + 1]; q++) {
+            const int j = g.items[q];
             double X = xq[3 * j + ind1], Y = xq[3 * j + ind2];
             // the reference's else-if chains: first matching column / row
             int col = -1, row = -1;
-            for (int c = 0; c < 6; c++)
-              if (fabs(cx[c] - X) < tol) {
-                col = c;
+            for (int cc = 0; cc < 6; cc++)
+              if (fabs(cx[cc] - X) < tol) {
+                col = cc;
                 break;
               }
             for (int r = 0; r < 6; r++)
@@ -369,10 +421,9 @@ Stencils build_stencils(double h, const double ctr[3], int nq, const double* xq,
           if (best >= 0) st[6 * a + bq] = best;
         }
     }
-    S.tgt.push_back(i);
-    for (int q = 0; q < 36; q++) S.idx.push_back(st[q]);
-    S.pq.push_back((X0[ind1] - xLow) / h);
-    S.pq.push_back((X0[ind2] - yLow) / h);
+    S.tgt[e] = i;
+    S.pq[2 * (size_t)e] = (X0[ind1] - xLow) / h;
+    S.pq[2 * (size_t)e + 1] = (X0[ind2] - yLow) / h;
   }
   return S;
 }
