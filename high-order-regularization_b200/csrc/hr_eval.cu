@@ -43,7 +43,11 @@ namespace {
 // reference's formulas (2S/utilities.cpp:211-254, :292-323) with ~1e-16
 // relative error; G(0) is the reference's r -> 0 value. The table of a kernel
 // family is staged in shared memory once per CTA.
-constexpr int kSmoothN = HR_SMOOTH_PIECES * (HR_SMOOTH_DEG + 2);
+constexpr int kSmoothN = HR_SMOOTH_PIECES * (HR_SMOOTH_DEG + 2);  // doubles per table (global)
+// shared-memory copy: each piece padded to an even length, read as double2
+constexpr int kSmoothW = HR_SMOOTH_DEG + 3;
+constexpr int kSmoothNs = HR_SMOOTH_PIECES * kSmoothW;
+static_assert(kSmoothW % 2 == 0, "a padded piece must be whole double2s");
 
 constexpr int kSmooth32N = HR_SMOOTH32_PIECES * 8;  // floats per FP32 table
 
@@ -60,20 +64,28 @@ __device__ __forceinline__ float smooth_eval_f(const float4* __restrict__ tab, f
   return fmaf(fmaf(fmaf(fmaf(fmaf(b.z, t, b.y), t, b.x), t, a.w), t, a.z), t, a.y);
 }
 
+// FP64 piece in shared memory: (centre, c0) (c1, c2) ... (c11, 0) as double2.
 __device__ __forceinline__ double smooth_eval(const double* __restrict__ tab, double s) {
   int i = (int)(sqrtf((float)s) * (HR_SMOOTH_PIECES / 8.0f));
   i = min(max(i, 0), HR_SMOOTH_PIECES - 1);
-  const double* p = tab + i * (HR_SMOOTH_DEG + 2);
-  const double t = s - p[0];
-  double v = p[HR_SMOOTH_DEG + 1];
+  const double2* p2 = reinterpret_cast<const double2*>(tab + i * kSmoothW);
+  double e[kSmoothW];
 #pragma unroll
-  for (int k = HR_SMOOTH_DEG; k >= 1; k--) v = fma(v, t, p[k]);
+  for (int k = 0; k < kSmoothW / 2; k++) {
+    const double2 v = p2[k];
+    e[2 * k] = v.x;
+    e[2 * k + 1] = v.y;
+  }
+  const double t = s - e[0];
+  double v = e[HR_SMOOTH_DEG + 1];
+#pragma unroll
+  for (int k = HR_SMOOTH_DEG; k >= 1; k--) v = fma(v, t, e[k]);
   return v;
 }
 
 constexpr int kWarps = kTB / 32;     // warps per CTA, each with its own tiles
 constexpr int kNT = 64;              // sources per (per-warp) shared-memory tile
-constexpr int kWarpSm = 10 * kNT;    // doubles per warp: 10 SoA arrays of a source tile
+constexpr int kWarpSm = 10 * kNT;    // doubles per warp: a source tile, 10 values per source
 constexpr int kSmem = kWarps * kWarpSm;
 constexpr int kMaxP1 = 16;
 
@@ -175,27 +187,22 @@ template <int KIND>
 __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, const Tgt& S,
                                        const Reg& g, const double* __restrict__ stab, double& a0,
                                        double& a1, double& a2) {
-  const double* X = sm;
-  const double* Y = sm + kNT;
-  const double* Z = sm + 2 * kNT;
-  const double* NX = sm + 3 * kNT;
-  const double* NY = sm + 4 * kNT;
-  const double* NZ = sm + 5 * kNT;
-  const double* A = sm + 6 * kNT;
-  const double* QX = sm + 7 * kNT;
-  const double* QY = sm + 8 * kNT;
-  const double* QZ = sm + 9 * kNT;
-  const double dx = S.px - X[j], dy = S.py - Y[j], dz = S.pz - Z[j];
+  // source j of the warp's tile: (x, y) (z, area) (nx, ny) (nz, qx) (qy, qz)
+  const double2* s2 = reinterpret_cast<const double2*>(sm) + 5 * j;
+  const double2 v0 = s2[0], v1 = s2[1], v2 = s2[2], v3 = s2[3], v4 = s2[4];
+  const double Xj = v0.x, Yj = v0.y, Zj = v1.x, Aj = v1.y;
+  const double NXj = v2.x, NYj = v2.y, NZj = v3.x, QXj = v3.y, QYj = v4.x, QZj = v4.y;
+  const double dx = S.px - Xj, dy = S.py - Yj, dz = S.pz - Zj;
   const double r2 = dx * dx + dy * dy + dz * dz;
   constexpr bool kTab = (KIND == K_SL_ON || KIND == K_DL_ON);  // tabulated smoothing, rsqrt only if r > 8 delta
   const double rinv = kTab ? 0.0 : rsqrt(r2);
   bool reg = false;
   if (KIND == K_SL_ON) {
     // Call_Ds_SL_onSurf (2S/KITC.cpp:807-846) with Stokes_SL_7ord_onSurf (2S/utilities.cpp:211)
-    const double area = A[j];
-    const double fx = QX[j] - S.f0n0 * NX[j];
-    const double fy = QY[j] - S.f0n0 * NY[j];
-    const double fz = QZ[j] - S.f0n0 * NZ[j];
+    const double area = Aj;
+    const double fx = QXj - S.f0n0 * NXj;
+    const double fy = QYj - S.f0n0 * NYj;
+    const double fz = QZj - S.f0n0 * NZj;
     const double fdd = fx * dx + fy * dy + fz * dz;
     double H1, H2;
     if (r2 > g.d64) {
@@ -205,7 +212,7 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     } else {
       const double sq = r2 * g.inv_d2;
       H1 = smooth_eval(stab, sq) * g.inv_d;
-      H2 = smooth_eval(stab + kSmoothN, sq) * g.inv_d3;
+      H2 = smooth_eval(stab + kSmoothNs, sq) * g.inv_d3;
       reg = r2 >= g.r0sq;
     }
     H1 *= area;
@@ -215,10 +222,10 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     a2 += fz * H1 + dz * H2;
   } else if ((KIND == K_SL_OFF || KIND == K_E2G_SL7) && S.near) {
     // Call_Ds_SL regularized branch (2S/KITC.cpp:847) / stokes_SL_7ord (E2G/stokes.cpp:53)
-    const double area = A[j];
-    const double fx = QX[j] - S.f0n0 * NX[j];
-    const double fy = QY[j] - S.f0n0 * NY[j];
-    const double fz = QZ[j] - S.f0n0 * NZ[j];
+    const double area = Aj;
+    const double fx = QXj - S.f0n0 * NXj;
+    const double fy = QYj - S.f0n0 * NYj;
+    const double fz = QZj - S.f0n0 * NZj;
     const double fdd = fx * dx + fy * dy + fz * dz;
     double H1, H2;
     reg = sl_7ord(r2, rinv, g, S.c, H1, H2);
@@ -229,20 +236,20 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     a2 += fz * H1 + dz * H2;
   } else if (KIND == K_SL_OFF || KIND == K_E2G_SL_AWAY) {
     // plain Stokeslet without subtraction (2S/KITC.cpp:856-882, E2G/stokes.cpp:22-40)
-    const double fx = QX[j], fy = QY[j], fz = QZ[j];
+    const double fx = QXj, fy = QYj, fz = QZj;
     const double fdd = fx * dx + fy * dy + fz * dz;
-    const double H1 = A[j] * rinv;
+    const double H1 = Aj * rinv;
     const double H2 = fdd * H1 * (rinv * rinv);
     a0 += fx * H1 + dx * H2;
     a1 += fy * H1 + dy * H2;
     a2 += fz * H1 + dz * H2;
   } else if (KIND == K_DL_ON) {
     // Call_Ds_DL_onSurf (2S/KITC.cpp:921-957)
-    const double gx = QX[j] - S.g0[0];
-    const double gy = QY[j] - S.g0[1];
-    const double gz = QZ[j] - S.g0[2];
+    const double gx = QXj - S.g0[0];
+    const double gy = QYj - S.g0[1];
+    const double gz = QZj - S.g0[2];
     const double gdd = gx * dx + gy * dy + gz * dz;
-    const double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+    const double ndd = NXj * dx + NYj * dy + NZj * dz;
     double H3;
     if (r2 > g.d64) {
       const double ri = rsqrt(r2), ri2 = ri * ri;
@@ -251,7 +258,7 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       H3 = smooth_eval(stab, r2 * g.inv_d2) * g.inv_d5;
       reg = r2 >= g.r0sq;
     }
-    const double kernel = ndd * gdd * H3 * A[j];
+    const double kernel = ndd * gdd * H3 * Aj;
     a0 += dx * kernel;
     a1 += dy * kernel;
     a2 += dz * kernel;
@@ -259,25 +266,25 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     if (S.near) {
       // Call_Ds_DL regularized branch (2S/KITC.cpp:996-1059), stokes_DL_7ord
       const double b = S.b;
-      const double xh0 = X[j] - S.x0[0];
-      const double xh1 = Y[j] - S.x0[1];
-      const double xh2 = Z[j] - S.x0[2];
-      const double gx = QX[j] - S.g0[0];
-      const double gy = QY[j] - S.g0[1];
-      const double gz = QZ[j] - S.g0[2];
+      const double xh0 = Xj - S.x0[0];
+      const double xh1 = Yj - S.x0[1];
+      const double xh2 = Zj - S.x0[2];
+      const double gx = QXj - S.g0[0];
+      const double gy = QYj - S.g0[1];
+      const double gz = QZj - S.g0[2];
       const double sig_sq = (xh0 * xh0 + xh1 * xh1 + xh2 * xh2) -
                             2.0 * b * (xh0 * S.n0[0] + xh1 * S.n0[1] + xh2 * S.n0[2]);
       const double g_dot_n0 = gx * S.n0[0] + gy * S.n0[1] + gz * S.n0[2];
       const double g_dot_xh = gx * xh0 + gy * xh1 + gz * xh2;
-      const double n0_dot_n = S.n0[0] * NX[j] + S.n0[1] * NY[j] + S.n0[2] * NZ[j];
-      const double xh_dot_n = xh0 * NX[j] + xh1 * NY[j] + xh2 * NZ[j];
+      const double n0_dot_n = S.n0[0] * NXj + S.n0[1] * NYj + S.n0[2] * NZj;
+      const double xh_dot_n = xh0 * NXj + xh1 * NYj + xh2 * NZj;
       const double c_m1a = g_dot_n0 * n0_dot_n;
       const double c_m1b = g_dot_xh * n0_dot_n + g_dot_n0 * xh_dot_n;
       const double c_m2a = g_dot_xh * xh_dot_n;
       const double c_m2b = b * c_m1b;
       double H2, H3;
       reg = dl_7ord(r2, rinv, g, S.c, H2, H3);
-      const double area = A[j];
+      const double area = Aj;
       H2 *= area;
       H3 *= area;
       double m1 = dx * c_m1a - S.n0[0] * c_m1b;
@@ -291,24 +298,24 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       a2 += m1 * H2 + m2 * H3;
     } else {
       // plain stresslet (2S/KITC.cpp:970-995)
-      const double gdd = QX[j] * dx + QY[j] * dy + QZ[j] * dz;
-      const double ndd = NX[j] * dx + NY[j] * dy + NZ[j] * dz;
+      const double gdd = QXj * dx + QYj * dy + QZj * dz;
+      const double ndd = NXj * dx + NYj * dy + NZj * dz;
       const double rinv2 = rinv * rinv;
-      const double kernel = gdd * ndd * (rinv2 * rinv2 * rinv) * A[j];
+      const double kernel = gdd * ndd * (rinv2 * rinv2 * rinv) * Aj;
       a0 += dx * kernel;
       a1 += dy * kernel;
       a2 += dz * kernel;
     }
   } else if (KIND == K_E2G_P_AWAY) {
     // stokes_pressure_away (E2G/stokes.cpp:108-121)
-    const double H2 = (QX[j] * dx + QY[j] * dy + QZ[j] * dz) * (rinv * rinv * rinv);
-    a0 += H2 * A[j];
+    const double H2 = (QXj * dx + QYj * dy + QZj * dz) * (rinv * rinv * rinv);
+    a0 += H2 * Aj;
   } else if (KIND == K_E2G_P7) {
     // stokes_pressure_7ord (E2G/stokes.cpp:151-194)
     double H2;
     reg = lapl_dl_7ord(r2, rinv, g, S.c, H2);
-    const double n0 = NX[j], n1 = NY[j], n2 = NZ[j];
-    const double f0 = QX[j], f1 = QY[j], f2 = QZ[j];
+    const double n0 = NXj, n1 = NYj, n2 = NZj;
+    const double f0 = QXj, f1 = QYj, f2 = QZj;
     const double f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
     const double ncf0 = (n1 * f2 - n2 * f1) - S.n0xf0[0];
     const double ncf1 = (n2 * f0 - n0 * f2) - S.n0xf0[1];
@@ -319,7 +326,7 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     const double ncd2 = n0 * dy - n1 * dx;
     const double normal = -(f_dot_n - S.f0n0) * n_dot_dx;
     const double tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
-    a0 += (normal + tangential) * H2 * A[j];
+    a0 += (normal + tangential) * H2 * Aj;
   }
   return reg;
 }
@@ -705,18 +712,13 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           const int s = s0 + i;
           const double x = T.sx[s], y = T.sy[s], z = T.sz[s];
           if (!kOn32) {
-            wsm[i] = x;
-            wsm[kNT + i] = y;
-            wsm[2 * kNT + i] = z;
-            if (kSrcNrm) {
-              wsm[3 * kNT + i] = T.snx[s];
-              wsm[4 * kNT + i] = T.sny[s];
-              wsm[5 * kNT + i] = T.snz[s];
-            }
-            wsm[6 * kNT + i] = T.sa[s];
-            wsm[7 * kNT + i] = T.qx[s];
-            wsm[8 * kNT + i] = T.qy[s];
-            wsm[9 * kNT + i] = T.qz[s];
+            double2* w2 = reinterpret_cast<double2*>(wsm) + 5 * i;
+            const double qx = T.qx[s];
+            w2[0] = make_double2(x, y);
+            w2[1] = make_double2(z, T.sa[s]);
+            w2[2] = kSrcNrm ? make_double2(T.snx[s], T.sny[s]) : make_double2(0.0, 0.0);
+            w2[3] = make_double2(kSrcNrm ? T.snz[s] : 0.0, qx);
+            w2[4] = make_double2(T.qy[s], T.qz[s]);
           }
           if (MIXED) {
             ws4[i] = make_float4((float)(x - cb[0]), (float)(y - cb[1]), (float)(z - cb[2]), T.fa[s]);
@@ -851,17 +853,22 @@ __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict
   __shared__ float chebf[kWarps * 3 * kMaxP1];
   __shared__ EvalTask sT;
   // smoothing tables: G1, G2 for the Stokeslet family, G3 for the stresslet family
-  __shared__ double stab[FAM == F_SL ? 2 * kSmoothN : (FAM == F_DL ? kSmoothN : 1)];
+  __shared__ __align__(16) double stab[FAM == F_SL ? 2 * kSmoothNs : (FAM == F_DL ? kSmoothNs : 2)];
   __shared__ float4 stab32[MIXED ? (FAM == F_SL ? 2 * kSmooth32N / 4 : (FAM == F_DL ? kSmooth32N / 4 : 1)) : 1];
   const BlockRef it = items[blockIdx.x];
   if (threadIdx.x == 0) sT = tasks[it.task];
-  if (FAM == F_SL) {
-    for (int i = threadIdx.x; i < kSmoothN; i += blockDim.x) {
-      stab[i] = kSmoothG1[i];
-      stab[kSmoothN + i] = kSmoothG2[i];
+  if (FAM == F_SL || FAM == F_DL) {
+    for (int i = threadIdx.x; i < kSmoothNs; i += blockDim.x) {
+      const int piece = i / kSmoothW, k = i - piece * kSmoothW;
+      const int src = piece * (HR_SMOOTH_DEG + 2) + k;
+      const bool pad = k == kSmoothW - 1;
+      if (FAM == F_SL) {
+        stab[i] = pad ? 0.0 : kSmoothG1[src];
+        stab[kSmoothNs + i] = pad ? 0.0 : kSmoothG2[src];
+      } else {
+        stab[i] = pad ? 0.0 : kSmoothG3[src];
+      }
     }
-  } else if (FAM == F_DL) {
-    for (int i = threadIdx.x; i < kSmoothN; i += blockDim.x) stab[i] = kSmoothG3[i];
   }
   if (MIXED && FAM != F_E2G) {
     float* t32 = reinterpret_cast<float*>(stab32);

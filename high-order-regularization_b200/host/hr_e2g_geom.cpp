@@ -256,24 +256,39 @@ void build(Scene& S, int N, double band1, double band2) {
         A[i2] = l2 * h + kCtr;
         B[i1] = l1 * h + kCtr;
         B[i2] = l2 * h + kCtr;
-        for (int j = -N; j <= N; j++) {
-          A[i] = j * h + kCtr;
-          B[i] = A[i] + h;
-          int sa = phi(A) < 0.0 ? -1 : 1, sb = phi(B) < 0.0 ? -1 : 1;
-          if (sa * sb < 0) {
-            double tau = newton(A, h, i, 0, 1);
-            double x[3] = {A[0], A[1], A[2]};
-            x[i] += tau * h;
-            double nv[3];
-            for (int k = 0; k < 3; k++) nv[k] = dphi(k, x);
-            double nn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-            for (int k = 0; k < 3; k++) nv[k] /= nn;
-            if (fabs(nv[i]) >= cth) {
-              double ar = h * h * part_unity(i, nv) / fabs(nv[i]);
-              out.insert(out.end(), {x[0], x[1], x[2], nv[0], nv[1], nv[2], ar});
+        // phi along the line is a quadratic in j, (j h / a_i)^2 + R: its sign
+        // can change only within a few segments of the roots +-j*. Rounding
+        // moves a sign change by far less than a segment, so the reference's
+        // scan of every segment (E2G/surface.cpp:26-64) is run over windows of
+        // 7 segments around the roots, in increasing j, with its own tests.
+        double y0[3] = {A[0], A[1], A[2]};
+        y0[i] = kCtr;
+        const double R = phi(y0);
+        if (R > 1e-10) continue;  // the line misses the surface
+        const double root = R < 0.0 ? sqrt(-R) * kAx[i] / h : 0.0;
+        const int ra = (int)floor(-root), rb = (int)floor(root);
+        const int lo1 = std::max(-N, ra - 3), hi1 = std::min(N, ra + 3);
+        const int lo2 = std::max(-N, std::max(rb - 3, hi1 + 1)), hi2 = std::min(N, rb + 3);
+        const int win[2][2] = {{lo1, hi1}, {lo2, hi2}};
+        for (const auto& wj : win)
+          for (int j = wj[0]; j <= wj[1]; j++) {
+            A[i] = j * h + kCtr;
+            B[i] = A[i] + h;
+            int sa = phi(A) < 0.0 ? -1 : 1, sb = phi(B) < 0.0 ? -1 : 1;
+            if (sa * sb < 0) {
+              double tau = newton(A, h, i, 0, 1);
+              double x[3] = {A[0], A[1], A[2]};
+              x[i] += tau * h;
+              double nv[3];
+              for (int k = 0; k < 3; k++) nv[k] = dphi(k, x);
+              double nn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+              for (int k = 0; k < 3; k++) nv[k] /= nn;
+              if (fabs(nv[i]) >= cth) {
+                double ar = h * h * part_unity(i, nv) / fabs(nv[i]);
+                out.insert(out.end(), {x[0], x[1], x[2], nv[0], nv[1], nv[2], ar});
+              }
             }
           }
-        }
       }
     }
   for (auto& v : per)
@@ -320,14 +335,30 @@ void build(Scene& S, int N, double band1, double band2) {
   std::vector<long> cand;
   for (long g = 0; g < M * M * M; g++)
     if (claim[g].load(std::memory_order_relaxed) < nq) cand.push_back(g);
-  // quadrature points bucketed by grid cell, for the retries below
-  std::vector<std::pair<long, int>> cells(nq);
-  auto cell_key = [&](long a, long b2, long c) { return (a * (M + 16) + b2) * (M + 16) + c; };
-  for (int q2 = 0; q2 < nq; q2++) {
-    const double* xs = &S.xq[3 * q2];
-    cells[q2] = {cell_key((long)floor(xs[0] / h) + 8, (long)floor(xs[1] / h) + 8, (long)floor(xs[2] / h) + 8), q2};
+  // quadrature points bucketed by grid cell (dense CSR table over the cells
+  // the surface occupies, ascending point index per cell), for the retries below
+  long cmin[3] = {0, 0, 0}, cmax[3] = {-1, -1, -1};
+  std::vector<long> qcell(3 * (size_t)nq);
+  for (int q2 = 0; q2 < nq; q2++)
+    for (int d = 0; d < 3; d++) {
+      const long c = (long)floor(S.xq[3 * q2 + d] / h);
+      qcell[3 * q2 + d] = c;
+      if (q2 == 0 || c < cmin[d]) cmin[d] = c;
+      if (q2 == 0 || c > cmax[d]) cmax[d] = c;
+    }
+  const long cn[3] = {cmax[0] - cmin[0] + 1, cmax[1] - cmin[1] + 1, cmax[2] - cmin[2] + 1};
+  auto cell_of = [&](long a, long b2, long c) -> long {
+    if (a < cmin[0] || a > cmax[0] || b2 < cmin[1] || b2 > cmax[1] || c < cmin[2] || c > cmax[2]) return -1;
+    return ((a - cmin[0]) * cn[1] + (b2 - cmin[1])) * cn[2] + (c - cmin[2]);
+  };
+  const long ncell = nq > 0 ? cn[0] * cn[1] * cn[2] : 0;
+  std::vector<int> cstart(ncell + 1, 0), citems(nq);
+  for (int q2 = 0; q2 < nq; q2++) cstart[cell_of(qcell[3 * q2], qcell[3 * q2 + 1], qcell[3 * q2 + 2]) + 1]++;
+  for (long c = 0; c < ncell; c++) cstart[c + 1] += cstart[c];
+  {
+    std::vector<int> fill(cstart.begin(), cstart.end() - 1);
+    for (int q2 = 0; q2 < nq; q2++) citems[fill[cell_of(qcell[3 * q2], qcell[3 * q2 + 1], qcell[3 * q2 + 2])]++] = q2;
   }
-  std::sort(cells.begin(), cells.end());
   std::vector<Tag> tags(cand.size());
   std::vector<uint8_t> ok(cand.size(), 0);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -352,10 +383,10 @@ void build(Scene& S, int N, double band1, double band2) {
       for (long a = i - 7; a <= i + 7; a++)
         for (long b2 = j - 7; b2 <= j + 7; b2++)
           for (long c2 = k - 7; c2 <= k + 7; c2++) {
-            long key = cell_key(a + 8, b2 + 8, c2 + 8);
-            auto it = std::lower_bound(cells.begin(), cells.end(), std::make_pair(key, -1));
-            for (; it != cells.end() && it->first == key; ++it) {
-              int q2 = it->second;
+            const long cell = cell_of(a, b2, c2);
+            if (cell < 0) continue;
+            for (int e = cstart[cell]; e < cstart[cell + 1]; e++) {
+              int q2 = citems[e];
               if (q2 <= t.q) continue;
               const double* xs = &S.xq[3 * q2];
               double d_sq = (pt[0] - xs[0]) * (pt[0] - xs[0]) + (pt[1] - xs[1]) * (pt[1] - xs[1]) +
@@ -377,20 +408,31 @@ void build(Scene& S, int N, double band1, double band2) {
       ok[c] = 1;
     }
   }
-  std::vector<Tag> kept;
+  // reference order: by claiming quadrature point, then the i, j, k loop. The
+  // candidates are in grid order, so a stable counting sort by q gives it.
+  std::vector<long> qstart(nq + 1, 0);
   for (size_t c = 0; c < cand.size(); c++)
-    if (ok[c]) kept.push_back(tags[c]);
-  // reference order: by claiming quadrature point, then the i, j, k loop
-  std::stable_sort(kept.begin(), kept.end(), [](const Tag& a, const Tag& b) {
-    return a.q != b.q ? a.q < b.q : a.g < b.g;
-  });
+    if (ok[c]) qstart[tags[c].q + 1]++;
+  for (int q2 = 0; q2 < nq; q2++) qstart[q2 + 1] += qstart[q2];
+  const long nkept = qstart[nq];
+  std::vector<Tag> kept(nkept);
+  for (size_t c = 0; c < cand.size(); c++)
+    if (ok[c]) kept[qstart[tags[c].q]++] = tags[c];
   S.nrst.assign(M * M * M, -1);
-  for (size_t t = 0; t < kept.size(); t++) {
-    S.nrst[kept[t].g] = (int)t;
-    S.b.push_back(kept[t].b);
-    S.x0.insert(S.x0.end(), {kept[t].x0[0], kept[t].x0[1], kept[t].x0[2]});
-    S.n0.insert(S.n0.end(), {kept[t].n0[0], kept[t].n0[1], kept[t].n0[2]});
-    S.band2.push_back(fabs(kept[t].b) <= band2 * h + tol ? 1 : 0);
+  S.b.resize(nkept);
+  S.x0.resize(3 * nkept);
+  S.n0.resize(3 * nkept);
+  S.band2.resize(nkept);
+#pragma omp parallel for schedule(static)
+  for (long t = 0; t < nkept; t++) {
+    const Tag& T = kept[t];
+    S.nrst[T.g] = (int)t;
+    S.b[t] = T.b;
+    for (int d = 0; d < 3; d++) {
+      S.x0[3 * t + d] = T.x0[d];
+      S.n0[3 * t + d] = T.n0[d];
+    }
+    S.band2[t] = fabs(T.b) <= band2 * h + tol ? 1 : 0;
   }
 }
 

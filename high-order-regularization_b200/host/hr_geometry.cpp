@@ -151,6 +151,49 @@ struct QPoint {
   int plane;
 };
 
+// Segments of grid line {A + t h e_i} (j = t) on which the reference's scan
+// (Generate_Surface, 2S/surface.cpp:26-66) can see a sign change of phi.
+// Along the line phi is the quadratic alpha j^2 + beta j + gamma (alpha > 0):
+// rounding (~1e-14 here) can flip its sign only where |phi| < 1e-13, i.e.
+// within a tiny distance of a real root or of the vertex of a quadratic whose
+// minimum is below 1e-12. Windows of 7 segments around the two roots (or the
+// vertex) keep every sign change; the scan runs over them in increasing j with
+// the reference's own tests. Returns false when the line misses the surface.
+bool line_windows(const Spheroid& S, const double* A, int i, double h, double off_i, int N, int lo[2],
+                  int hi[2]) {
+  double x0[3] = {A[0], A[1], A[2]};
+  x0[i] = off_i;
+  if (S.centered)
+    for (int k = 0; k < 3; k++) x0[k] -= S.ctr[k];
+  double u0[3], r[3];
+  for (int k = 0; k < 3; k++) {
+    if (S.rotated) {
+      u0[k] = S.R[k][0] * x0[0] + S.R[k][1] * x0[1] + S.R[k][2] * x0[2];
+      r[k] = S.R[k][i];
+    } else {
+      u0[k] = x0[k];
+      r[k] = k == i ? 1.0 : 0.0;
+    }
+  }
+  double alpha = 0.0, beta = 0.0, gamma = -1.0;
+  for (int k = 0; k < 3; k++) {
+    alpha += h * h * r[k] * r[k] / S.a2[k];
+    beta += 2.0 * h * u0[k] * r[k] / S.a2[k];
+    gamma += u0[k] * u0[k] / S.a2[k];
+  }
+  const double v = -beta / (2.0 * alpha);
+  const double minval = gamma - beta * beta / (4.0 * alpha);
+  if (minval > 1e-12) return false;
+  const double half = sqrt(std::max(0.0, -minval / alpha));
+  const int ra = (int)std::max(-1e9, std::min(1e9, floor(v - half)));
+  const int rb = (int)std::max(-1e9, std::min(1e9, floor(v + half)));
+  lo[0] = std::max(-N, ra - 3);
+  hi[0] = std::min(N, ra + 3);
+  lo[1] = std::max(-N, std::max(rb - 3, hi[0] + 1));
+  hi[1] = std::min(N, rb + 3);
+  return true;
+}
+
 // Generate_Surface: 2S/surface.cpp:13-71 (grid at origin + offset; points
 // translated by shift afterwards).
 std::vector<QPoint> generate_surface(const Spheroid& S, int N, double h, const double off[3],
@@ -168,27 +211,30 @@ std::vector<QPoint> generate_surface(const Spheroid& S, int N, double h, const d
         A[i2] = l2 * h + off[i2];
         B[i1] = l1 * h + off[i1];
         B[i2] = l2 * h + off[i2];
-        for (int j = -N; j <= N; j++) {
-          A[i] = j * h + off[i];
-          B[i] = A[i] + h;
-          int sa = S.phi(A) < 0.0 ? -1 : 1, sb = S.phi(B) < 0.0 ? -1 : 1;
-          if (sa * sb < 0) {
-            double tau = newton(S, A, h, i, 0, 1);
-            QPoint q;
-            q.x[0] = A[0];
-            q.x[1] = A[1];
-            q.x[2] = A[2];
-            q.x[i] += tau * h;
-            for (int k = 0; k < 3; k++) q.n[k] = S.dphi(k, q.x);
-            double nn = sqrt(q.n[0] * q.n[0] + q.n[1] * q.n[1] + q.n[2] * q.n[2]);
-            for (int k = 0; k < 3; k++) q.n[k] /= nn;
-            if (fabs(q.n[i]) >= cth) {
-              q.area = h * h * part_unity(i, q.n) / fabs(q.n[i]);
-              q.plane = i;
-              out.push_back(q);
+        int lo[2], hi[2];
+        if (!line_windows(S, A, i, h, off[i], N, lo, hi)) continue;  // the line misses the surface
+        for (int w = 0; w < 2; w++)
+          for (int j = lo[w]; j <= hi[w]; j++) {
+            A[i] = j * h + off[i];
+            B[i] = A[i] + h;
+            int sa = S.phi(A) < 0.0 ? -1 : 1, sb = S.phi(B) < 0.0 ? -1 : 1;
+            if (sa * sb < 0) {
+              double tau = newton(S, A, h, i, 0, 1);
+              QPoint q;
+              q.x[0] = A[0];
+              q.x[1] = A[1];
+              q.x[2] = A[2];
+              q.x[i] += tau * h;
+              for (int k = 0; k < 3; k++) q.n[k] = S.dphi(k, q.x);
+              double nn = sqrt(q.n[0] * q.n[0] + q.n[1] * q.n[1] + q.n[2] * q.n[2]);
+              for (int k = 0; k < 3; k++) q.n[k] /= nn;
+              if (fabs(q.n[i]) >= cth) {
+                q.area = h * h * part_unity(i, q.n) / fabs(q.n[i]);
+                q.plane = i;
+                out.push_back(q);
+              }
             }
           }
-        }
       }
     }
   }
@@ -396,9 +442,16 @@ struct CellIndex {
       }
     }
   }
-  int nearest(const std::vector<QPoint>& P, const double* pt, int f) const {
+  // The point of family f nearest to pt (squared distance below 100), the
+  // lowest index among equals: the reference's linear scan
+  // (2S/surface.cpp:370-390). The answer does not depend on the order in which
+  // points are met, so the cell closest to pt is scanned first, then every
+  // cell whose box can still hold a point as close (box distances carry a
+  // 1e-12 relative margin for rounding).
+  int nearest(const std::vector<QPoint>& P, const double* pt, int f, std::vector<double>& d2c) const {
     const int nc = (int)members[f].size();
-    std::vector<std::pair<double, int>> order(nc);
+    d2c.resize(nc);
+    int c0 = -1;
     for (int c = 0; c < nc; c++) {
       const double* b = &box[f][6 * c];
       double d2 = 0;
@@ -408,14 +461,13 @@ struct CellIndex {
         else if (pt[k] > b[2 * k + 1]) d = pt[k] - b[2 * k + 1];
         d2 += d * d;
       }
-      order[c] = {d2, c};
+      d2c[c] = d2;
+      if (c0 < 0 || d2 < d2c[c0]) c0 = c;
     }
-    std::sort(order.begin(), order.end());
     int i0 = -1;
     double best = 100.0;
-    for (auto& oc : order) {
-      if (oc.first > best * (1.0 + 1e-12) + 1e-300) break;
-      for (int j : members[f][oc.second]) {
+    auto scan = [&](int c) {
+      for (int j : members[f][c]) {
         const double* x = P[j].x;
         double dist = (pt[0] - x[0]) * (pt[0] - x[0]) + (pt[1] - x[1]) * (pt[1] - x[1]) +
                       (pt[2] - x[2]) * (pt[2] - x[2]);
@@ -424,7 +476,11 @@ struct CellIndex {
           i0 = j;
         }
       }
-    }
+    };
+    if (c0 < 0) return -1;
+    scan(c0);
+    for (int c = 0; c < nc; c++)
+      if (c != c0 && d2c[c] <= best * (1.0 + 1e-12) + 1e-300) scan(c);
     return i0;
   }
 };
@@ -530,10 +586,11 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
     G->i123[t].assign(3 * n, 0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int i = 0; i < n; i++) {
+      thread_local std::vector<double> d2c;
       const double* pt = P[t][i].x;
       int i1, i2, i3;
       monge(S, pt, i1, i2, i3);
-      int nrst_i = CI.nearest(P[src], pt, i3);
+      int nrst_i = CI.nearest(P[src], pt, i3, d2c);
       G->nrst[t][i] = nrst_i;
       if (nrst_i < 0) continue;
       double x0[3], n0[3];
