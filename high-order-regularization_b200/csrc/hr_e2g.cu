@@ -87,6 +87,32 @@ __device__ void grid_exact(int N, double h, long g, double& p, double u[3]) {
   }
 }
 
+// Mid-plane j = N/2 (y = 1.5) slices: extended p, |p - p_exact|, |u - u_exact|
+// and p_exact, the last three outside or on the surface only (0 inside), as
+// the reference's slice files (E2G/main.cpp:221-224, 297-300, 505-546).
+__global__ void midplane_kernel(int N, double h, const double* __restrict__ p, const double* __restrict__ u,
+                                double* __restrict__ out) {
+  const long M = N + 1, m3 = M * M * M, mm = M * M;
+  const long e = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= mm) return;
+  const int i = (int)(e / M), k = (int)(e % M), j = N / 2;
+  const long g = ((long)i * M + j) * M + k;
+  const double x = i * h, y = j * h, z = k * h;
+  const double lv = (x - 1.5) * (x - 1.5) + (y - 1.5) * (y - 1.5) / 0.25 + (z - 1.5) * (z - 1.5) / 0.25 - 1.0;
+  double pe = 0.0, dp = 0.0, du = 0.0;
+  if (lv > 0.0 || fabs(lv) < 1e-12) {
+    double ue[3];
+    exact_pu(x, y, z, pe, ue);
+    dp = fabs(p[g] - pe);
+    const double d0 = u[g] - ue[0], d1 = u[m3 + g] - ue[1], d2 = u[2 * m3 + g] - ue[2];
+    du = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+  }
+  out[e] = p[g];
+  out[mm + e] = dp;
+  out[2 * mm + e] = du;
+  out[3 * mm + e] = pe;
+}
+
 constexpr int kErrBlocks = 148 * 4, kErrThreads = 256, kErrVals = 12;
 
 // Per-block maxima and sums (fixed grid-stride assignment, so the final
@@ -201,6 +227,7 @@ struct hr_e2g {
   DBuf<double> p_bi, u_bi, p_ext, u_ext;  // grids
   DBuf<double> p_ref, u_ref;              // snapshot of the extended grids for comparisons
   bool have_ref = false;
+  bool ran = false;                       // hr_e2g_run has filled the grids
   Batch batch[3];                         // by precision: FP64, mixed, all FP32
   long long pairs = 0;
   PoissonWork* pw = nullptr;              // FFT plan and grid buffers of the four Poisson solves
@@ -374,6 +401,7 @@ extern "C" int hr_e2g_run(hr_e2g* E, int precision, hr_e2g_report* rep) {
     HR_CHECK_CUDA(cudaEventRecord(ev[0], st));
     HR_REQUIRE(precision == HR_FP64 || precision == HR_MIXED || precision == HR_FP32, "unknown precision");
     E->batch[precision].launch(C);
+    E->ran = true;
     HR_CHECK_CUDA(cudaEventRecord(ev[1], st));
     // grids: p = 0, u = (1, 0, 0) off the evaluated points (E2G/main.cpp:1062, 1234-1236)
     int fb = 148 * 8;
@@ -491,6 +519,28 @@ extern "C" int hr_e2g_snapshot(hr_e2g* E) {
     HR_CHECK_CUDA(cudaStreamSynchronize(st));
     E->have_ref = true;
   } catch (const hr::Error& e) {
+    C.err = e.what();
+    return e.code;
+  }
+  return HR_OK;
+}
+
+extern "C" int hr_e2g_midplane(hr_e2g* E, double* out) {
+  if (!E || !out) return HR_ERR_ARG;
+  Ctx& C = E->owner->c;
+  try {
+    cudaStream_t st = C.stream;
+    if (!E->ran) throw Error(HR_ERR_STATE, "hr_e2g_midplane needs a completed hr_e2g_run");
+    const int N = E->S.N;
+    const long M = N + 1, mm = M * M;
+    DBuf<double> d;
+    d.alloc(4 * (size_t)mm);
+    midplane_kernel<<<(unsigned)((mm + 255) / 256), 256, 0, st>>>(N, E->S.h, E->p_ext.p, E->u_ext.p, d.p);
+    C.launches++;
+    HR_CHECK_CUDA(cudaGetLastError());
+    HR_CHECK_CUDA(cudaMemcpyAsync(out, d.p, sizeof(double) * 4 * mm, cudaMemcpyDeviceToHost, st));
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+  } catch (const Error& e) {
     C.err = e.what();
     return e.code;
   }

@@ -398,6 +398,15 @@ def gmres_opts(restart=15, max_iter=100, tol=1e-10, precision=HR_FP64, use_guess
     return o
 
 
+def write_npy(path, a):
+    """Writes a float64 array as a .npy file through the library's writer (hr_write_npy)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    shape = (ctypes.c_longlong * max(1, a.ndim))(*(a.shape or (1,)))
+    rc = lib().hr_write_npy(str(path).encode(), _dp(a), max(1, a.ndim), shape)
+    if rc != HR_OK:
+        raise HrError(rc, "hr_write_npy failed for %s" % path)
+
+
 class Plan2S:
     """Device-resident two-surface problem (trees, lists, stencils uploaded once)."""
 
@@ -551,6 +560,14 @@ class E2G:
         out = np.zeros(3 * m if which in (1, 3) else m)
         self.ctx._check(lib().hr_e2g_get(self.p, which, _dp(out)))
         return out
+
+    def midplane(self):
+        """Mid-plane y = 1.5 slices of the last run, shape (4, N+1, N+1) in (i, k) order:
+        extended p, |p - p_exact|, |u - u_exact| (0 inside the body) and p_exact (0 inside)."""
+        M = self.N + 1
+        out = np.zeros(4 * M * M)
+        self.ctx._check(lib().hr_e2g_midplane(self.p, _dp(out)))
+        return out.reshape(4, M, M)
 
     def scene(self):
         nq, nt = self.info["nq"], self.info["n_tagged"]

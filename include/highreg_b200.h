@@ -410,6 +410,18 @@ int hr_stokeslet_away_noalloc(const double* xyz_src_dev, const double* area_dev,
                               const double* xyz_tgt_dev, int nt, double* out_dev, void* stream);
 long long hr_stokeslet_away_noalloc_max_targets(void);
 
+/* ------------------------------------------------------------ output */
+/* Writes a float64 array as a NumPy .npy file (version 1.0, little-endian, C
+ * order), the binary form of the reference's text dumps (vel1 / vel2,
+ * 2S/main.cpp:258-270; mid-plane slices, E2G/main.cpp:115-118). */
+int hr_write_npy(const char* path, const double* data, int ndim, const long long* shape);
+/* Mid-plane y = 1.5 (j = N/2) slices of the last hr_e2g_run, gathered on the
+ * device (the reference's p_midY / err_p_midY / err_u_midY files,
+ * E2G/main.cpp:297-300, 546): out holds 4 x (N+1)^2 doubles in (i, k) order:
+ * extended p; |p - p_exact| outside or on the surface (0 inside); |u -
+ * u_exact| likewise; p_exact likewise. */
+int hr_e2g_midplane(hr_e2g* e, double* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -100,6 +100,16 @@ def test_exact_solution_error_table_h32(ctx):
     assert abs(d["band_u_max"] - be.max()) <= 1e-12 * be.max()
     assert abs(d["band_u_rms"] - np.sqrt(np.mean(be ** 2))) <= 1e-9 * d["band_u_rms"]
     assert d["ref_u_rel_l2"] == -1.0
+    # mid-plane y = 1.5 slices gathered on the device (the reference's slice files)
+    M, jm = N + 1, N // 2
+    sl = e.midplane()
+    out_mid = outside.reshape(M, M, M)[:, jm, :]
+    assert np.array_equal(sl[0], p.reshape(M, M, M)[:, jm, :])
+    # the device and host exact solutions differ by rounding (~1e-16 of |p|, |u| = O(1)),
+    # which the error slices see as an absolute difference
+    for q, ref in ((1, perr), (2, uerr), (3, pex)):
+        want = np.where(out_mid, ref.reshape(M, M, M)[:, jm, :], 0.0)
+        assert np.allclose(sl[q], want, rtol=1e-12, atol=1e-13), q
     # precision variants against the FP64 grids and the exact solution
     e.snapshot()
     for prec, tol in ((highreg.HR_MIXED, 1e-7), (highreg.HR_FP32, 1e-3)):
