@@ -370,7 +370,7 @@ def run_ours(args, rank, world, local_rank):
     # (trees, interaction lists, stencils) + RHS + solve + solution read back
     e2e_times, plan_times = [], []
     h2d = sum(np.asarray(v).nbytes for k, v in geo.items() if isinstance(v, np.ndarray))
-    for _ in range(max(1, min(args.steps, 3))):
+    for _ in range(max(1, min(args.steps, 5 if H_INV <= 64 else 3))):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         p2 = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=P, N0=N0, theta=THETA)

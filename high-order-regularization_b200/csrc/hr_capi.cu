@@ -221,6 +221,9 @@ extern "C" int hr_ctx_create(int device, hr_ctx** out) {
     ctx->c.num_sms = prop.multiProcessorCount;
     HR_CHECK_CUDA(cudaSetDevice(device));
     HR_CHECK_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+    HR_CHECK_CUDA(cudaStreamCreateWithFlags(&ctx->c.side, cudaStreamNonBlocking));
+    HR_CHECK_CUDA(cudaEventCreateWithFlags(&ctx->c.ev_fork, cudaEventDisableTiming));
+    HR_CHECK_CUDA(cudaEventCreateWithFlags(&ctx->c.ev_join, cudaEventDisableTiming));
     ctx->c.counters.alloc(64);
     ctx->c.counters.zero(ctx->c.stream);
   });
@@ -232,11 +235,17 @@ extern "C" int hr_ctx_create(int device, hr_ctx** out) {
 extern "C" void hr_ctx_destroy(hr_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->c.device);
+  if (ctx->c.side) {
+    cudaStreamSynchronize(ctx->c.side);
+    cudaStreamDestroy(ctx->c.side);
+  }
   if (ctx->c.stream) {
     cudaStreamSynchronize(ctx->c.stream);
     ctx->c.counters.release();
     cudaStreamDestroy(ctx->c.stream);
   }
+  if (ctx->c.ev_fork) cudaEventDestroy(ctx->c.ev_fork);
+  if (ctx->c.ev_join) cudaEventDestroy(ctx->c.ev_join);
   delete ctx;
 }
 
@@ -446,13 +455,13 @@ struct hr_plan2s {
 
 namespace {
 
-// Stresslet batches of the matvec, one per precision from prec0 on, over the
-// given trees and lists (the plan's own, or the inner operator's).
-void dl_batches(hr_plan2s& P, DevTree* tree, DevLists* Lon, DevLists* Loff, Batch* dl, int prec0,
+// Stresslet batches of the matvec, one per precision in [prec0, prec1), over
+// the given trees and lists (the plan's own, or the inner operator's).
+void dl_batches(hr_plan2s& P, DevTree* tree, DevLists* Lon, DevLists* Loff, Batch* dl, int prec0, int prec1,
                 bool count) {
   cudaStream_t st = P.C->stream;
   const bool direct = P.opt.mode == HR_DIRECT;
-  for (int prec = prec0; prec < 3; prec++) {
+  for (int prec = prec0; prec < prec1; prec++) {
     Batch& B = dl[prec];
     B.family = F_DL;
     B.tasks.clear();
@@ -485,7 +494,8 @@ void plan_batches(hr_plan2s& P) {
   cudaStream_t st = P.C->stream;
   P.counters.alloc(4 * 8);
   P.counters.zero(st);
-  dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, true);
+  // the reduced-precision batches are built on first use (plan_matvec)
+  dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, 1, true);
   Batch& B = P.sl;
   B.family = F_SL;
   for (int t = 0; t < 2; t++) {
@@ -521,6 +531,7 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
                   P.xin.p + P.off[1 - t], P.tg[t].g0.p, st);
     C.launches++;
   }
+  if (!in && !P.dl[prec].ready) dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, prec, prec + 1, true);
   (in ? in->dl[prec] : P.dl[prec]).launch(C);
   // set 0: u - on*f - comp*f ; set 1: u - comp*f - on*f   (2S/main.cpp:612-676)
   launch_matvec_combine(3 * P.nq[0], 2.0 / 3.0, P.xin.p + P.off[0], P.out_on[0].p, P.out_off[0].p,
@@ -865,7 +876,7 @@ extern "C" int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double t
       in->Lon[t].build(in->tree[t].host, Q.nq[t], Q.surf_host[t].xyz, all.data(), st);
       in->Loff[t].build(in->tree[1 - t].host, Q.nq[t], Q.surf_host[t].xyz, Q.near_host[t].data(), st);
     }
-    dl_batches(Q, in->tree, in->Lon, in->Loff, in->dl, 1, false);
+    dl_batches(Q, in->tree, in->Lon, in->Loff, in->dl, 1, 3, false);
     // accuracy of the inner operator (mixed precision) against the plan's FP64
     // one, on a fixed pseudo-random density
     Q.inner.reset();
@@ -1122,6 +1133,7 @@ extern "C" int hr_plan2s_time_batch(hr_plan2s* plan, int which, int iters, doubl
   return guard(ctx_of(plan), [&] {
     cudaStream_t st = plan->C->stream;
     HR_REQUIRE(which != 3 || plan->inner, "the plan has no inner treecode");
+    if (which == 2 && !plan->dl[1].ready) dl_batches(*plan, plan->tree, plan->Lon, plan->Loff, plan->dl, 1, 2, true);
     Batch& B = which == 3 ? plan->inner->dl[1] : which == 1 ? plan->sl : plan->dl[which == 2 ? 1 : 0];
     cudaEvent_t a, b;
     HR_CHECK_CUDA(cudaEventCreate(&a));

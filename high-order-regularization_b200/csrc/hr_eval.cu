@@ -842,10 +842,14 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   }
 }
 
-template <int FAM, bool MIXED>
-__global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict__ tasks,
-                                                      const BlockRef* __restrict__ items,
-                                                      const Seg* __restrict__ segs) {
+// ON = true: the batch's on-surface items only (K_SL_ON / K_DL_ON). Their code
+// path needs fewer registers than the off-surface kinds' (no nearest-point
+// data, no per-target regularization coefficients), so it runs with five
+// resident CTAs per SM instead of four.
+template <int FAM, bool MIXED, bool ON>
+__global__ void __launch_bounds__(kTB, ON ? 5 : 4) eval_kernel(const EvalTask* __restrict__ tasks,
+                                                               const BlockRef* __restrict__ items,
+                                                               const Seg* __restrict__ segs) {
   __shared__ __align__(16) double sm[kSmem];
   // per-warp FP32 source tiles: (x, y, z, area), (n, 0), (q, 0) per source
   __shared__ float4 sf[MIXED ? kWarps * 3 * kNT : 1];
@@ -884,10 +888,10 @@ __global__ void __launch_bounds__(kTB, 4) eval_kernel(const EvalTask* __restrict
   __syncthreads();
   const int kind = sT.kind;
   if (FAM == F_SL) {
-    if (kind == K_SL_ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    if (ON) run_item<K_SL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_SL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else if (FAM == F_DL) {
-    if (kind == K_DL_ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    if (ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else {
     switch (kind) {
@@ -961,18 +965,39 @@ __global__ void __launch_bounds__(kTB) reduce_kernel(const EvalTask* __restrict_
 
 }  // namespace
 
+template <int FAM, bool MIXED>
+void launch_family(const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs, int nitems, int n_on,
+                   cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
+  if constexpr (FAM != F_E2G) {
+    const bool two = n_on > 0 && nitems > n_on && side;
+    if (two) {
+      cudaEventRecord(fork, st);
+      cudaStreamWaitEvent(side, fork, 0);
+    }
+    if (n_on > 0) eval_kernel<FAM, MIXED, true><<<n_on, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+    if (nitems > n_on)
+      eval_kernel<FAM, MIXED, false><<<nitems - n_on, kTB, 0, two ? side : st>>>(d_tasks, d_items + n_on, d_segs);
+    if (two) {
+      cudaEventRecord(join, side);
+      cudaStreamWaitEvent(st, join, 0);
+    }
+  } else {
+    eval_kernel<FAM, MIXED, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+  }
+}
+
 void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs,
-                 int nitems, int ntask_blocks, const int2* d_task_blocks, cudaStream_t st,
-                 bool mixed) {
+                 int nitems, int n_on, int ntask_blocks, const int2* d_task_blocks, cudaStream_t st,
+                 cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, bool mixed) {
   if (nitems > 0) {
     if (!mixed) {
-      if (family == F_SL) eval_kernel<F_SL, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
-      else if (family == F_DL) eval_kernel<F_DL, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
-      else eval_kernel<F_E2G, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+      if (family == F_SL) launch_family<F_SL, false>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
+      else if (family == F_DL) launch_family<F_DL, false>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
+      else launch_family<F_E2G, false>(d_tasks, d_items, d_segs, nitems, 0, st, side, fork, join);
     } else {
-      if (family == F_SL) eval_kernel<F_SL, true><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
-      else if (family == F_DL) eval_kernel<F_DL, true><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
-      else eval_kernel<F_E2G, true><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+      if (family == F_SL) launch_family<F_SL, true>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
+      else if (family == F_DL) launch_family<F_DL, true>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
+      else launch_family<F_E2G, true>(d_tasks, d_items, d_segs, nitems, 0, st, side, fork, join);
     }
   }
   if (ntask_blocks > 0) reduce_kernel<<<ntask_blocks, kTB, 0, st>>>(d_tasks, d_task_blocks);

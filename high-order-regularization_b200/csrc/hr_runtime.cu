@@ -67,9 +67,16 @@ void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direc
   }
   // upward-pass items: every non-root node (the root's moments stay zero, as
   // in the reference, which skips it: 2S/KITC.cpp:1446), in chunks of sources.
+  // Chunks of at most 512 sources, smaller when the tree is small so that the
+  // items fill about four CTAs per SM (a multiple of the 32-source K tile).
   std::vector<MomItem> it;
   std::vector<int> start(nn + 1, 0);
-  const int chunk = 512;
+  long long members = 0;
+  for (int c = 1; c < nn; c++) members += host.m1[c] - host.m0[c] + 1;
+  int sms = 148, dev = 0;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long want = (members + 4LL * sms - 1) / (4LL * sms);
+  const int chunk = (int)std::min(512LL, std::max(64LL, (want + 31) / 32 * 32));
   moment_terms = 0;
   for (int c = 0; c < nn; c++) {
     start[c] = (int)it.size();
@@ -275,12 +282,23 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
     }
     starts.push_back(slot);
   }
+  // on-surface items first (their own launch), each part by decreasing cost
+  auto on_kind = [&](const BlockRef& r) {
+    const int k = tasks[r.task].kind;
+    return family != F_E2G && (k == K_SL_ON || k == K_DL_ON);
+  };
   std::stable_sort(items.begin(), items.end(),
-                   [](const std::pair<double, BlockRef>& a, const std::pair<double, BlockRef>& b) {
+                   [&](const std::pair<double, BlockRef>& a, const std::pair<double, BlockRef>& b) {
+                     const bool oa = on_kind(a.second), ob = on_kind(b.second);
+                     if (oa != ob) return oa;
                      return a.first > b.first;
                    });
   std::vector<BlockRef> br(items.size());
-  for (size_t i = 0; i < items.size(); i++) br[i] = items[i].second;
+  n_on = 0;
+  for (size_t i = 0; i < items.size(); i++) {
+    br[i] = items[i].second;
+    n_on += on_kind(br[i]) ? 1 : 0;
+  }
   nitems = (int)br.size();
   ntask_blocks = (int)tblocks.size();
   d_items.upload(br, st);
@@ -293,12 +311,13 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
     tasks[t].partial = d_partial.p;
   }
   d_tasks.upload(tasks, st);
+  ready = true;
 }
 
 void Batch::launch(Ctx& C) {
-  launch_eval(family, d_tasks.p, d_items.p, d_segs.p, nitems, ntask_blocks, d_task_blocks.p,
-              C.stream, !tasks.empty() && tasks[0].mixed);
-  C.launches += 2;
+  launch_eval(family, d_tasks.p, d_items.p, d_segs.p, nitems, n_on, ntask_blocks, d_task_blocks.p,
+              C.stream, C.side, C.ev_fork, C.ev_join, !tasks.empty() && tasks[0].mixed);
+  C.launches += 1 + (n_on > 0 ? 1 : 0) + (nitems > n_on ? 1 : 0);
 }
 
 }  // namespace hr

@@ -77,6 +77,10 @@ struct DBuf {
 struct Ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // a second stream forked from and joined back to `stream` around the two
+  // launches of a boundary-sum batch, so that each fills the other's tail
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string err;
   long long launches = 0;
   int num_sms = 148;
@@ -132,7 +136,8 @@ struct DevStencils {
   void build(const Stencils& S, cudaStream_t st);
 };
 
-// A batch of boundary sums evaluated in one launch.
+// A batch of boundary sums evaluated together (one or two kernel launches and
+// one reduction).
 struct Batch {
   int family = F_SL;
   std::vector<EvalTask> tasks;
@@ -145,6 +150,8 @@ struct Batch {
   DBuf<int2> d_task_blocks;
   DBuf<double> d_partial;
   int nitems = 0, ntask_blocks = 0;
+  int n_on = 0;  // leading items of on-surface tasks (launched on their own)
+  bool ready = false;  // finalize has run
   // builds the segments and cost-balanced work items of all tasks
   void finalize(cudaStream_t st, int num_sms = 148);
   void launch(Ctx& C);
