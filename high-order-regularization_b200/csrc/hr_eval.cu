@@ -198,8 +198,8 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
   const double rinv = kTab ? 0.0 : rsqrt(r2);
   bool reg = false;
   if (KIND == K_SL_ON) {
-    // Call_Ds_SL_onSurf (2S/KITC.cpp:807-846) with Stokes_SL_7ord_onSurf (2S/utilities.cpp:211)
-    const double area = Aj;
+    // Call_Ds_SL_onSurf (2S/KITC.cpp:807-846) with Stokes_SL_7ord_onSurf (2S/utilities.cpp:211);
+    // the tile holds area x density and area x normal for this kind, so f is area x (f - f0n0 n)
     const double fx = QXj - S.f0n0 * NXj;
     const double fy = QYj - S.f0n0 * NYj;
     const double fz = QZj - S.f0n0 * NZj;
@@ -211,12 +211,11 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       H2 = ri * ri * ri;
     } else {
       const double sq = r2 * g.inv_d2;
-      H1 = smooth_eval(stab, sq) * g.inv_d;
-      H2 = smooth_eval(stab + kSmoothNs, sq) * g.inv_d3;
+      H1 = smooth_eval(stab, sq);
+      H2 = smooth_eval(stab + kSmoothNs, sq);
       reg = r2 >= g.r0sq;
     }
-    H1 *= area;
-    H2 *= area * fdd;
+    H2 *= fdd;
     a0 += fx * H1 + dx * H2;
     a1 += fy * H1 + dy * H2;
     a2 += fz * H1 + dz * H2;
@@ -244,7 +243,7 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     a1 += fy * H1 + dy * H2;
     a2 += fz * H1 + dz * H2;
   } else if (KIND == K_DL_ON) {
-    // Call_Ds_DL_onSurf (2S/KITC.cpp:921-957)
+    // Call_Ds_DL_onSurf (2S/KITC.cpp:921-957); the tile holds area x normal for this kind
     const double gx = QXj - S.g0[0];
     const double gy = QYj - S.g0[1];
     const double gz = QZj - S.g0[2];
@@ -255,10 +254,10 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       const double ri = rsqrt(r2), ri2 = ri * ri;
       H3 = ri2 * ri2 * ri;
     } else {
-      H3 = smooth_eval(stab, r2 * g.inv_d2) * g.inv_d5;
+      H3 = smooth_eval(stab, r2 * g.inv_d2);
       reg = r2 >= g.r0sq;
     }
-    const double kernel = ndd * gdd * H3 * Aj;
+    const double kernel = ndd * gdd * H3;
     a0 += dx * kernel;
     a1 += dy * kernel;
     a2 += dz * kernel;
@@ -414,16 +413,16 @@ __device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, 
     const float fdd = fx * dx + fy * dy + fz * dz;
     float H1, H2;
     if (sq <= 64.0f) {
-      H1 = smooth_eval_f(tab, sq) * gf.inv_d;
-      H2 = smooth_eval_f(tab + kSmooth32N / 4, sq) * gf.inv_d3;
+      H1 = smooth_eval_f(tab, sq);
+      H2 = smooth_eval_f(tab + kSmooth32N / 4, sq);
     } else {
       H1 = rsqrtf(r2);
       H2 = H1 * H1 * H1;
     }
-    const float h1 = H1 * P.w, h2 = H2 * P.w * fdd;
-    p0 += fx * h1 + dx * h2;
-    p1 += fy * h1 + dy * h2;
-    p2 += fz * h1 + dz * h2;
+    const float h2 = H2 * fdd;  // the tile holds area x density and area x normal
+    p0 += fx * H1 + dx * h2;
+    p1 += fy * H1 + dy * h2;
+    p2 += fz * H1 + dz * h2;
   } else {  // K_DL_ON
     const float gx = Q.x - F.g0[0];
     const float gy = Q.y - F.g0[1];
@@ -432,12 +431,12 @@ __device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, 
     const float ndd = N.x * dx + N.y * dy + N.z * dz;
     float H3;
     if (sq <= 64.0f) {
-      H3 = smooth_eval_f(tab, sq) * gf.inv_d5;
+      H3 = smooth_eval_f(tab, sq);
     } else {
       const float ri = rsqrtf(r2), ri2 = ri * ri;
       H3 = ri2 * ri2 * ri;
     }
-    const float kernel = ndd * gdd * H3 * P.w;
+    const float kernel = ndd * gdd * H3;  // the tile holds area x normal
     p0 += dx * kernel;
     p1 += dy * kernel;
     p2 += dz * kernel;
@@ -711,19 +710,32 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
         for (int i = lane; i < cnt; i += 32) {
           const int s = s0 + i;
           const double x = T.sx[s], y = T.sy[s], z = T.sz[s];
+          // on-surface kinds: area folded into the normal (and, for the
+          // Stokeslet, the density), which they only use multiplied by it
+          constexpr bool kAreaN = (KIND == K_SL_ON || KIND == K_DL_ON), kAreaQ = (KIND == K_SL_ON);
           if (!kOn32) {
             double2* w2 = reinterpret_cast<double2*>(wsm) + 5 * i;
-            const double qx = T.qx[s];
+            const double as = T.sa[s];
+            const double an = kAreaN ? as : 1.0, aq = kAreaQ ? as : 1.0;
             w2[0] = make_double2(x, y);
-            w2[1] = make_double2(z, T.sa[s]);
-            w2[2] = kSrcNrm ? make_double2(T.snx[s], T.sny[s]) : make_double2(0.0, 0.0);
-            w2[3] = make_double2(kSrcNrm ? T.snz[s] : 0.0, qx);
-            w2[4] = make_double2(T.qy[s], T.qz[s]);
+            w2[1] = make_double2(z, as);
+            w2[2] = kSrcNrm ? make_double2(an * T.snx[s], an * T.sny[s]) : make_double2(0.0, 0.0);
+            w2[3] = make_double2(kSrcNrm ? an * T.snz[s] : 0.0, aq * T.qx[s]);
+            w2[4] = make_double2(aq * T.qy[s], aq * T.qz[s]);
           }
           if (MIXED) {
             ws4[i] = make_float4((float)(x - cb[0]), (float)(y - cb[1]), (float)(z - cb[2]), T.fa[s]);
-            if (kSrcNrm) ws4[kNT + i] = make_float4(T.fnx[s], T.fny[s], T.fnz[s], 0.f);
-            ws4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
+            if (kAreaN) {
+              const double as = T.sa[s];
+              ws4[kNT + i] = make_float4((float)(as * T.snx[s]), (float)(as * T.sny[s]), (float)(as * T.snz[s]), 0.f);
+              if (kAreaQ)
+                ws4[2 * kNT + i] = make_float4((float)(as * T.qx[s]), (float)(as * T.qy[s]), (float)(as * T.qz[s]), 0.f);
+              else
+                ws4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
+            } else {
+              if (kSrcNrm) ws4[kNT + i] = make_float4(T.fnx[s], T.fny[s], T.fnz[s], 0.f);
+              ws4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
+            }
           }
         }
         __syncwarp();
@@ -861,27 +873,32 @@ __global__ void __launch_bounds__(kTB, ON ? 5 : 4) eval_kernel(const EvalTask* _
   __shared__ float4 stab32[MIXED ? (FAM == F_SL ? 2 * kSmooth32N / 4 : (FAM == F_DL ? kSmooth32N / 4 : 1)) : 1];
   const BlockRef it = items[blockIdx.x];
   if (threadIdx.x == 0) sT = tasks[it.task];
-  if (FAM == F_SL || FAM == F_DL) {
+  // The tables carry the powers of 1/delta of the factors they give: the
+  // coefficients (not the piece centres) are scaled by 1/delta, 1/delta^3
+  // (G1, G2) or 1/delta^5 (G3) while they are staged.
+  if ((FAM == F_SL || FAM == F_DL) && ON) {
+    const Reg gs = make_reg(tasks[it.task].DEL);
     for (int i = threadIdx.x; i < kSmoothNs; i += blockDim.x) {
       const int piece = i / kSmoothW, k = i - piece * kSmoothW;
       const int src = piece * (HR_SMOOTH_DEG + 2) + k;
       const bool pad = k == kSmoothW - 1;
       if (FAM == F_SL) {
-        stab[i] = pad ? 0.0 : kSmoothG1[src];
-        stab[kSmoothNs + i] = pad ? 0.0 : kSmoothG2[src];
+        stab[i] = pad ? 0.0 : kSmoothG1[src] * (k == 0 ? 1.0 : gs.inv_d);
+        stab[kSmoothNs + i] = pad ? 0.0 : kSmoothG2[src] * (k == 0 ? 1.0 : gs.inv_d3);
       } else {
-        stab[i] = pad ? 0.0 : kSmoothG3[src];
+        stab[i] = pad ? 0.0 : kSmoothG3[src] * (k == 0 ? 1.0 : gs.inv_d5);
       }
     }
-  }
-  if (MIXED && FAM != F_E2G) {
-    float* t32 = reinterpret_cast<float*>(stab32);
-    for (int i = threadIdx.x; i < kSmooth32N; i += blockDim.x) {
-      if (FAM == F_SL) {
-        t32[i] = kSmooth32G1[i];
-        t32[kSmooth32N + i] = kSmooth32G2[i];
-      } else {
-        t32[i] = kSmooth32G3[i];
+    if (MIXED) {
+      float* t32 = reinterpret_cast<float*>(stab32);
+      for (int i = threadIdx.x; i < kSmooth32N; i += blockDim.x) {
+        const bool centre = (i & 7) == 0;
+        if (FAM == F_SL) {
+          t32[i] = kSmooth32G1[i] * (centre ? 1.0f : (float)gs.inv_d);
+          t32[kSmooth32N + i] = kSmooth32G2[i] * (centre ? 1.0f : (float)gs.inv_d3);
+        } else {
+          t32[i] = kSmooth32G3[i] * (centre ? 1.0f : (float)gs.inv_d5);
+        }
       }
     }
   }
