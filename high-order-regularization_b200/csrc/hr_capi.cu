@@ -992,8 +992,23 @@ extern "C" int hr_plan2s_solve(hr_plan2s* plan, const hr_gmres_opts* opt, const 
 }
 
 extern "C" int hr_plan2s_work(hr_plan2s* plan, int which, hr_work* w) {
-  if (!plan || !w) return HR_ERR_ARG;
+  if (!plan || !w || which < 0 || which > 2) return HR_ERR_ARG;
   return guard(ctx_of(plan), [&] {
+    if (which == 2) {
+      // the inner treecode's stresslet batch, from its interaction lists (no launch)
+      if (!plan->inner) throw Error(HR_ERR_STATE, "the plan has no inner treecode");
+      const hr_plan2s::Inner& in = *plan->inner;
+      memset(w, 0, sizeof(*w));
+      for (int t = 0; t < 2; t++)
+        for (const DevLists* L : {&in.Lon[t], &in.Loff[t]}) {
+          w->direct_pairs_near += L->host.near_pairs_reg;
+          w->direct_pairs_far += L->host.near_pairs_plain;
+          w->proxy_pairs += L->host.proxy_pairs;
+        }
+      for (int s = 0; s < 2; s++) w->moment_terms += in.tree[s].moment_terms;
+      w->flops = 0;  // the r <= 8 delta split of the direct pairs is only counted by a launch
+      return;
+    }
     cudaStream_t st = plan->C->stream;
     plan->counters.zero(st);
     DBuf<double> tmp;

@@ -454,6 +454,8 @@ class Plan2S:
         return x, rep.as_dict()
 
     def work(self, which=0):
+        """Work counts: 0 one matvec (counted by a launch), 1 the RHS, 2 the inner
+        treecode's stresslet batch (from its lists; flops 0)."""
         w = Work()
         self.ctx._check(lib().hr_plan2s_work(self.p, which, ctypes.byref(w)))
         return w.as_dict()

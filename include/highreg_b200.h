@@ -257,7 +257,11 @@ typedef struct {
   long long moment_terms;      /* proxy x source terms of the upward pass */
   long long flops;             /* algorithmic flops by the fixed per-pair convention */
 } hr_work;
-int hr_plan2s_work(hr_plan2s* plan, int which /*0 matvec, 1 rhs*/, hr_work* w);
+/* which 2: the inner treecode's stresslet batch (hr_plan2s_set_inner_tree),
+ * counted from its interaction lists without a launch: direct pairs of
+ * regularized-branch targets in direct_pairs_near, of the others in
+ * direct_pairs_far; flops is 0. */
+int hr_plan2s_work(hr_plan2s* plan, int which /*0 matvec, 1 rhs, 2 inner*/, hr_work* w);
 /* Self-check of the reduced-precision upward pass: for density x (host, n),
  * the proxy moments of both trees from the tensor-core 3xTF32 kernel against
  * the FP64 ones; max over nodes and channels of max |difference| / max |FP64
