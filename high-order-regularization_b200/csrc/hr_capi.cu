@@ -856,6 +856,7 @@ extern "C" int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double t
   return guard(plan->owner, [&] {
     hr_plan2s& Q = *plan;
     HR_REQUIRE(Q.opt.mode == HR_TREE, "an inner treecode needs an HR_TREE plan");
+    if (rel_err) *rel_err = 0.0;
     if (P == 0) {
       HR_CHECK_CUDA(cudaStreamSynchronize(Q.C->stream));
       Q.inner.reset();
