@@ -363,7 +363,7 @@ def run_ours(args, rank, world, local_rank):
         # dram__bytes_read.sum + dram__bytes_write.sum of this launch from one ncu capture
         # (profiles/eval_kernel_fp64_stresslet_h64.md): sources are staged once per tile, so
         # DRAM traffic is tiny next to the compute; the bound is the FP64 pipe
-        roofline["traffic"] = 16167680 + 1762304
+        roofline["traffic"] = 10836992 + 157952 + 10935808 + 0
         roofline["traffic_source"] = "ncu capture of this kernel at this workload"
 
     # end to end through the C ABI with host buffers: scene upload + plan

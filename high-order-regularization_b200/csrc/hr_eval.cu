@@ -205,7 +205,7 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     const double fz = QZj - S.f0n0 * NZj;
     const double fdd = fx * dx + fy * dy + fz * dz;
     double H1, H2;
-    if (r2 > g.d64) {
+    if (r2 > g.dplain) {
       const double ri = rsqrt(r2);
       H1 = ri;
       H2 = ri * ri * ri;
@@ -213,8 +213,8 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       const double sq = r2 * g.inv_d2;
       H1 = smooth_eval(stab, sq);
       H2 = smooth_eval(stab + kSmoothNs, sq);
-      reg = r2 >= g.r0sq;
     }
+    reg = r2 <= g.d64 && r2 >= g.r0sq;  // the reference's branch (work counters)
     H2 *= fdd;
     a0 += fx * H1 + dx * H2;
     a1 += fy * H1 + dy * H2;
@@ -250,13 +250,13 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
     const double gdd = gx * dx + gy * dy + gz * dz;
     const double ndd = NXj * dx + NYj * dy + NZj * dz;
     double H3;
-    if (r2 > g.d64) {
+    if (r2 > g.dplain) {
       const double ri = rsqrt(r2), ri2 = ri * ri;
       H3 = ri2 * ri2 * ri;
     } else {
       H3 = smooth_eval(stab, r2 * g.inv_d2);
-      reg = r2 >= g.r0sq;
     }
+    reg = r2 <= g.d64 && r2 >= g.r0sq;  // the reference's branch (work counters)
     const double kernel = ndd * gdd * H3;
     a0 += dx * kernel;
     a1 += dy * kernel;
@@ -412,7 +412,7 @@ __device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, 
     const float fz = Q.z - F.f0n0 * N.z;
     const float fdd = fx * dx + fy * dy + fz * dz;
     float H1, H2;
-    if (sq <= 64.0f) {
+    if (sq <= kPlainOnSurf32) {
       H1 = smooth_eval_f(tab, sq);
       H2 = smooth_eval_f(tab + kSmooth32N / 4, sq);
     } else {
@@ -430,7 +430,7 @@ __device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, 
     const float gdd = gx * dx + gy * dy + gz * dz;
     const float ndd = N.x * dx + N.y * dy + N.z * dz;
     float H3;
-    if (sq <= 64.0f) {
+    if (sq <= kPlainOnSurf32) {
       H3 = smooth_eval_f(tab, sq);
     } else {
       const float ri = rsqrtf(r2), ri2 = ri * ri;

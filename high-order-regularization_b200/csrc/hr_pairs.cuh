@@ -26,9 +26,18 @@ struct Coef {
 };
 
 // Per-target constants of the regularized kernels.
+// Beyond r = sqrt(51) delta (r/delta = 7.14) the on-surface smoothing factors
+// G1, G2, G3 equal the singular kernel's to a relative 2^-54 (their erfc and
+// polynomial-times-Gaussian terms are smaller; 7.11 is the largest of the three
+// thresholds), so the FP64 sums take the plain kernel there; below 28.5 delta^2
+// (r/delta = 5.34) the same holds to 2^-25 for the FP32 sums.
+constexpr double kPlainOnSurf64 = 51.0;
+constexpr float kPlainOnSurf32 = 28.5f;
+
 struct Reg {
   double d, inv_d, d64, r0sq;  // delta, 1/delta, 64 delta^2, (1e-14)^2
   double inv_d2, inv_d3, inv_d5;
+  double dplain;               // kPlainOnSurf64 delta^2
 };
 
 __device__ __forceinline__ Reg make_reg(double d) {
@@ -40,6 +49,7 @@ __device__ __forceinline__ Reg make_reg(double d) {
   g.inv_d2 = g.inv_d * g.inv_d;
   g.inv_d3 = g.inv_d2 * g.inv_d;
   g.inv_d5 = g.inv_d3 * g.inv_d2;
+  g.dplain = kPlainOnSurf64 * d * d;
   return g;
 }
 
