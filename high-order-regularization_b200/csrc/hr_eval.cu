@@ -398,11 +398,9 @@ __device__ __forceinline__ void pair32(const float4* __restrict__ s4, int j, con
 // the singular kernel beyond (a branch that only warps at the 8 delta
 // boundary split on).
 template <int KIND>
-__device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, const Tgt32& F, const RegF& gf,
-                                          const float4* __restrict__ tab, float& p0, float& p1, float& p2) {
-  const float4 P = s4[j];  // x, y, z, area
-  const float4 N = s4[kNT + j];
-  const float4 Q = s4[2 * kNT + j];
+__device__ __forceinline__ void pair32tab_src(const float4& P, const float4& N, const float4& Q, const Tgt32& F,
+                                              const RegF& gf, const float4* __restrict__ tab, float& p0, float& p1,
+                                              float& p2) {
   const float dx = F.px - P.x, dy = F.py - P.y, dz = F.pz - P.z;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float sq = r2 * gf.inv_d2;
@@ -441,6 +439,13 @@ __device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, 
     p1 += dy * kernel;
     p2 += dz * kernel;
   }
+}
+
+template <int KIND>
+__device__ __forceinline__ void pair32tab(const float4* __restrict__ s4, int j, const Tgt32& F, const RegF& gf,
+                                          const float4* __restrict__ tab, float& p0, float& p1, float& p2) {
+  // source j: (x, y, z, area), area x normal, density (area x density for the Stokeslet)
+  pair32tab_src<KIND>(s4[j], s4[kNT + j], s4[2 * kNT + j], F, gf, tab, p0, p1, p2);
 }
 
 // ------------------------------------------------ FP32 pairs, r > 3 delta
@@ -854,6 +859,224 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   }
 }
 
+// ------------------------------------- two targets per thread (mixed, on-surface)
+
+// FP32 proxies of a run of Chebyshev rows for two targets: each shared-memory
+// read of a proxy serves both. Sums per row go to acc (FP64).
+template <bool DL>
+__device__ __forceinline__ void proxies32_rows2(const float4* __restrict__ s4, int row0, int nrows, int P1,
+                                                const float* __restrict__ chebf, const Tgt32 (&F)[2],
+                                                double (&acc)[2][3]) {
+  constexpr int W = DL ? 3 : 2;  // float4 per proxy
+  for (int r = 0; r < nrows; r++) {
+    const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
+    const float cx = chebf[pi], cy = chebf[P1 + pj];
+    float d0[2], d1[2], r01[2], d00[2], d11[2], d01[2], g0r[2];
+    float p[2][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      d0[q] = F[q].px - cx;
+      d1[q] = F[q].py - cy;
+      r01[q] = d0[q] * d0[q] + d1[q] * d1[q];
+      d00[q] = d0[q] * d0[q];
+      d11[q] = d1[q] * d1[q];
+      d01[q] = d0[q] * d1[q];
+      g0r[q] = F[q].g0[0] * d0[q] + F[q].g0[1] * d1[q];
+    }
+    const float4* row = s4 + r * P1 * W;
+    for (int pk = 0; pk < P1; pk++) {
+      const float cz = chebf[2 * P1 + pk];
+      const float4 A = row[pk * W];
+      const float4 B = row[pk * W + 1];
+      const float Cx = DL ? reinterpret_cast<const float*>(row + pk * W + 2)[0] : 0.f;
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const float d2 = F[q].pz - cz;
+        const float rinv = rsqrtf(fmaf(d2, d2, r01[q]));
+        if (DL) {
+          const float dmd = A.x * d00[q] + A.y * d11[q] + A.z * (d2 * d2) + A.w * d01[q] + B.x * (d0[q] * d2) +
+                            B.y * (d1[q] * d2);
+          const float mnd = B.z * d0[q] + B.w * d1[q] + Cx * d2;
+          const float g0d = fmaf(F[q].g0[2], d2, g0r[q]);
+          const float ri2 = rinv * rinv;
+          const float kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
+          p[q][0] += d0[q] * kernel;
+          p[q][1] += d1[q] * kernel;
+          p[q][2] += d2 * kernel;
+        } else {
+          const float m0 = A.x - F[q].f0n0 * A.w;
+          const float m1 = A.y - F[q].f0n0 * B.x;
+          const float m2 = A.z - F[q].f0n0 * B.y;
+          const float temp = (m0 * d0[q] + m1 * d1[q] + m2 * d2) * (rinv * rinv * rinv);
+          p[q][0] += m0 * rinv + temp * d0[q];
+          p[q][1] += m1 * rinv + temp * d1[q];
+          p[q][2] += m2 * rinv + temp * d2;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+      for (int c = 0; c < 3; c++) acc[q][c] += (double)p[q][c];
+  }
+}
+
+// The reduced-precision on-surface items (K_SL_ON / K_DL_ON, every pair in
+// FP32 with the tabulated smoothing factors) with two targets per thread: a
+// CTA of kTB2 = 64 threads covers the block's 128 targets — warp w holds
+// targets 64 w + lane and 64 w + 32 + lane, i.e. mask words 2 w and 2 w + 1 —
+// so every source and proxy read from shared memory serves two pairs.
+constexpr int kTB2 = 64;
+template <int KIND>
+__device__ __forceinline__ void run_item_on2(const EvalTask& T, const BlockRef& it, const Seg* __restrict__ segs,
+                                             double* sm, float4* s4, float* chebf, const float4* stab32) {
+  constexpr bool DL = (KIND == K_DL_ON);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int blk = it.blk;
+  double cb[3];
+  {
+    const int t0 = T.tord[blk * kTB];
+    cb[0] = T.txyz[3 * t0];
+    cb[1] = T.txyz[3 * t0 + 1];
+    cb[2] = T.txyz[3 * t0 + 2];
+  }
+  Tgt32 F[2];
+  bool valid[2];
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int k = blk * kTB + warp * 64 + q * 32 + lane;
+    valid[q] = k < T.nt;
+    Tgt S;
+    load_target<KIND>(T, valid[q] ? T.tord[k] : 0, valid[q], cb, S, F[q]);
+  }
+  const Reg g = make_reg(T.DEL);
+  RegF gf;
+  gf.inv_d = (float)g.inv_d;
+  gf.d64 = (float)g.d64;
+  gf.inv_d2 = (float)g.inv_d2;
+  gf.inv_d3 = (float)g.inv_d3;
+  gf.inv_d5 = (float)g.inv_d5;
+  double a[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+  double* wsm = sm + warp * kWarpSm;
+  float4* ws4 = s4 + warp * 3 * kNT;
+  float* wchebf = chebf + warp * 3 * kMaxP1;
+  for (int qs = it.seg0; qs < it.seg1; qs++) {
+    const Seg sg = segs[qs];
+    const Entry E = T.entries[sg.entry];
+    const uint32_t mA = E.mask[2 * warp], mB = E.mask[2 * warp + 1];
+    if ((mA | mB) == 0u) continue;
+    const bool actA = valid[0] && ((mA >> lane) & 1u);
+    const bool actB = valid[1] && ((mB >> lane) & 1u);
+    if (E.type == 1) {
+      const int m0 = sg.s0, m1 = sg.s1 - 1;
+      for (int s0 = m0; s0 <= m1; s0 += kNT) {
+        const int cnt = min(kNT, m1 - s0 + 1);
+        __syncwarp();
+        for (int i = lane; i < cnt; i += 32) {
+          const int s = s0 + i;
+          const double as = T.sa[s];
+          ws4[i] = make_float4((float)(T.sx[s] - cb[0]), (float)(T.sy[s] - cb[1]), (float)(T.sz[s] - cb[2]),
+                               (float)as);
+          ws4[kNT + i] = make_float4((float)(as * T.snx[s]), (float)(as * T.sny[s]), (float)(as * T.snz[s]), 0.f);
+          if (KIND == K_SL_ON)
+            ws4[2 * kNT + i] = make_float4((float)(as * T.qx[s]), (float)(as * T.qy[s]), (float)(as * T.qz[s]), 0.f);
+          else
+            ws4[2 * kNT + i] = make_float4(T.fqx[s], T.fqy[s], T.fqz[s], 0.f);
+        }
+        __syncwarp();
+        if (!actA && !actB) continue;
+        for (int j0 = 0; j0 < cnt; j0 += 16) {
+          float pA[3] = {0.f, 0.f, 0.f}, pB[3] = {0.f, 0.f, 0.f};
+          const int j1 = min(cnt, j0 + 16);
+#pragma unroll 2
+          for (int j = j0; j < j1; j++) {
+            const float4 P = ws4[j], N = ws4[kNT + j], Q = ws4[2 * kNT + j];
+            pair32tab_src<KIND>(P, N, Q, F[0], gf, stab32, pA[0], pA[1], pA[2]);
+            pair32tab_src<KIND>(P, N, Q, F[1], gf, stab32, pB[0], pB[1], pB[2]);
+          }
+          if (actA)
+            for (int c = 0; c < 3; c++) a[0][c] += (double)pA[c];
+          if (actB)
+            for (int c = 0; c < 3; c++) a[1][c] += (double)pB[c];
+        }
+      }
+    } else {
+      // far node: the proxy-major FP32 moments through the warp's tile, double-buffered
+      const int P1 = T.P1, Pf = T.Pf;
+      constexpr int kBpp = DL ? 48 : 32;  // bytes per proxy
+      constexpr int kHalf = kWarpSm * 4;  // bytes per buffer
+      const char* src = reinterpret_cast<const char*>(T.momf + (size_t)E.node * Pf * (DL ? 12 : 8));
+      char* buf = reinterpret_cast<char*>(wsm);
+      const int rowb = P1 * kBpp;
+      const int nr = max(1, kHalf / rowb);
+      const int nrow_all = P1 * P1;
+      const int nch = (nrow_all + nr - 1) / nr;
+      __syncwarp();
+      for (int i = lane; i < 3 * P1; i += 32)
+        wchebf[i] = (float)(T.tcheb[(size_t)E.node * 3 * P1 + i] - cb[i / P1]);
+      warp_copy_async(buf, src, min(nr, nrow_all) * rowb, lane);
+      double acc[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+      for (int ch = 0; ch < nch; ch++) {
+        const int row0 = ch * nr, rows = min(nr, nrow_all - row0);
+        if (ch + 1 < nch) {
+          const int r1 = row0 + nr;
+          warp_copy_async(buf + ((ch + 1) & 1) * kHalf, src + (size_t)r1 * rowb, min(nr, nrow_all - r1) * rowb,
+                          lane);
+          copy_async_wait<1>();
+        } else {
+          copy_async_wait<0>();
+        }
+        __syncwarp();
+        if (actA || actB)
+          proxies32_rows2<DL>(reinterpret_cast<const float4*>(buf + (ch & 1) * kHalf), row0, rows, P1, wchebf, F,
+                              acc);
+        __syncwarp();
+      }
+      if (actA)
+        for (int c = 0; c < 3; c++) a[0][c] += acc[0][c];
+      if (actB)
+        for (int c = 0; c < 3; c++) a[1][c] += acc[1][c];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    double* o = T.partial + ((size_t)it.slot * kTB + warp * 64 + q * 32 + lane) * 3;
+    o[0] = a[q][0];
+    o[1] = a[q][1];
+    o[2] = a[q][2];
+  }
+}
+
+template <int FAM>
+__global__ void __launch_bounds__(kTB2, 8) eval_kernel_on2(const EvalTask* __restrict__ tasks,
+                                                           const BlockRef* __restrict__ items,
+                                                           const Seg* __restrict__ segs) {
+  constexpr int kW2 = kTB2 / 32;
+  __shared__ __align__(16) double sm[kW2 * kWarpSm];
+  __shared__ float4 sf[kW2 * 3 * kNT];
+  __shared__ float chebf[kW2 * 3 * kMaxP1];
+  __shared__ EvalTask sT;
+  __shared__ float4 stab32[FAM == F_SL ? 2 * kSmooth32N / 4 : kSmooth32N / 4];
+  const BlockRef it = items[blockIdx.x];
+  if (threadIdx.x == 0) sT = tasks[it.task];
+  {
+    // FP32 tables with the powers of 1/delta in the coefficients (as in eval_kernel)
+    const Reg gs = make_reg(tasks[it.task].DEL);
+    float* t32 = reinterpret_cast<float*>(stab32);
+    for (int i = threadIdx.x; i < kSmooth32N; i += blockDim.x) {
+      const bool centre = (i & 7) == 0;
+      if (FAM == F_SL) {
+        t32[i] = kSmooth32G1[i] * (centre ? 1.0f : (float)gs.inv_d);
+        t32[kSmooth32N + i] = kSmooth32G2[i] * (centre ? 1.0f : (float)gs.inv_d3);
+      } else {
+        t32[i] = kSmooth32G3[i] * (centre ? 1.0f : (float)gs.inv_d5);
+      }
+    }
+  }
+  __syncthreads();
+  if (FAM == F_SL) run_item_on2<K_SL_ON>(sT, it, segs, sm, sf, chebf, stab32);
+  else run_item_on2<K_DL_ON>(sT, it, segs, sm, sf, chebf, stab32);
+}
+
 // ON = true: the batch's on-surface items only (K_SL_ON / K_DL_ON). Their code
 // path needs fewer registers than the off-surface kinds' (no nearest-point
 // data, no per-target regularization coefficients), so it runs with five
@@ -991,7 +1214,10 @@ void launch_family(const EvalTask* d_tasks, const BlockRef* d_items, const Seg* 
       cudaEventRecord(fork, st);
       cudaStreamWaitEvent(side, fork, 0);
     }
-    if (n_on > 0) eval_kernel<FAM, MIXED, true><<<n_on, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+    if (n_on > 0) {
+      if constexpr (MIXED) eval_kernel_on2<FAM><<<n_on, kTB2, 0, st>>>(d_tasks, d_items, d_segs);
+      else eval_kernel<FAM, MIXED, true><<<n_on, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+    }
     if (nitems > n_on)
       eval_kernel<FAM, MIXED, false><<<nitems - n_on, kTB, 0, two ? side : st>>>(d_tasks, d_items + n_on, d_segs);
     if (two) {

@@ -69,6 +69,8 @@ def _exact_grids(N, h):
 def test_exact_solution_error_table_h32(ctx):
     """E2G N = 96: the reference's own error table (the survey's golden values)."""
     e = highreg.E2G(ctx, 96)
+    with pytest.raises(highreg.HrError):  # no slices before a run
+        e.midplane()
     info = e.info
     assert info["nq"] == 6958 and info["n_tagged"] == 44582 and info["n_band"] == 26810 and info["n_face"] == 55298
     e.run()

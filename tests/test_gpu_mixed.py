@@ -121,8 +121,13 @@ def test_inner_tree_solve_reaches_fp64_residual(ctx, geo32):
     assert ri["matvecs_mixed"] > 0
     assert ri["true_residual"] <= 1e-10
     assert rel_err(xi, x64) < 1e-8
+    # its work, counted from its interaction lists
+    w = p.work(2)
+    assert w["direct_pairs_near"] > 0 and w["proxy_pairs"] > 0 and w["moment_terms"] > 0
     # removing it restores the plan's own operator
     assert p.set_inner_tree(0, 0) == 0.0
+    with pytest.raises(highreg.HrError):
+        p.work(2)
     p.matvec_dev(ut, yi, highreg.HR_MIXED)
     torch.cuda.synchronize()
     assert rel_err(yi.cpu().numpy(), ym.cpu().numpy()) == 0.0
