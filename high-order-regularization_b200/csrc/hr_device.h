@@ -63,11 +63,11 @@ struct BlockRef {
 
 enum Family : int { F_SL = 0, F_DL = 1, F_E2G = 2 };
 
-// Evaluates every work item of a combined list — the first n_on items (those
-// of on-surface tasks) in one launch on st, the rest in another on `side`
-// (forked from and joined back to st with the two events; on st as well when
-// side is null) — then reduces the partial sums per target (deterministic
-// order) and applies the epilogue.
+// Evaluates every work item of a combined list — the first n_on items (lean:
+// on-surface tasks, or the extend-to-grid box-face sums) in one launch on st,
+// the rest in another on `side` (forked from and joined back to st with the
+// two events; on st as well when side is null) — then reduces the partial sums
+// per target (deterministic order) and applies the epilogue.
 void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs,
                  int nitems, int n_on, int ntask_blocks, const int2* d_task_blocks, cudaStream_t st,
                  cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, bool mixed);

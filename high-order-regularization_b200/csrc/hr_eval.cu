@@ -1077,14 +1077,15 @@ __global__ void __launch_bounds__(kTB2, 8) eval_kernel_on2(const EvalTask* __res
   else run_item_on2<K_DL_ON>(sT, it, segs, sm, sf, chebf, stab32);
 }
 
-// ON = true: the batch's on-surface items only (K_SL_ON / K_DL_ON). Their code
-// path needs fewer registers than the off-surface kinds' (no nearest-point
+// ON = true: the batch's lean items only — on-surface kinds (K_SL_ON / K_DL_ON)
+// or, for the extend-to-grid family, the plain box-face sums (K_E2G_*_AWAY).
+// Their code path needs fewer registers than the others' (no nearest-point
 // data, no per-target regularization coefficients), so it runs with five
-// resident CTAs per SM instead of four.
+// (box-face sums: six) resident CTAs per SM instead of four.
 template <int FAM, bool MIXED, bool ON>
-__global__ void __launch_bounds__(kTB, ON ? 5 : 4) eval_kernel(const EvalTask* __restrict__ tasks,
-                                                               const BlockRef* __restrict__ items,
-                                                               const Seg* __restrict__ segs) {
+__global__ void __launch_bounds__(kTB, ON ? (FAM == F_E2G ? 6 : 5) : 4)
+    eval_kernel(const EvalTask* __restrict__ tasks, const BlockRef* __restrict__ items,
+                const Seg* __restrict__ segs) {
   __shared__ __align__(16) double sm[kSmem];
   // per-warp FP32 source tiles: (x, y, z, area), (n, 0), (q, 0) per source
   __shared__ float4 sf[MIXED ? kWarps * 3 * kNT : 1];
@@ -1133,13 +1134,12 @@ __global__ void __launch_bounds__(kTB, ON ? 5 : 4) eval_kernel(const EvalTask* _
   } else if (FAM == F_DL) {
     if (ON) run_item<K_DL_ON, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_DL_OFF, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
-  } else {
-    switch (kind) {
-      case K_E2G_SL_AWAY: run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
-      case K_E2G_P_AWAY: run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
-      case K_E2G_SL7: run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
-      default: run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32); break;
-    }
+  } else if (ON) {  // extend-to-grid: the plain box-face sums
+    if (kind == K_E2G_SL_AWAY) run_item<K_E2G_SL_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    else run_item<K_E2G_P_AWAY, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+  } else {  // extend-to-grid: the regularized band sums
+    if (kind == K_E2G_SL7) run_item<K_E2G_SL7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    else run_item<K_E2G_P7, MIXED>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   }
 }
 
@@ -1208,24 +1208,20 @@ __global__ void __launch_bounds__(kTB) reduce_kernel(const EvalTask* __restrict_
 template <int FAM, bool MIXED>
 void launch_family(const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs, int nitems, int n_on,
                    cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
-  if constexpr (FAM != F_E2G) {
-    const bool two = n_on > 0 && nitems > n_on && side;
-    if (two) {
-      cudaEventRecord(fork, st);
-      cudaStreamWaitEvent(side, fork, 0);
-    }
-    if (n_on > 0) {
-      if constexpr (MIXED) eval_kernel_on2<FAM><<<n_on, kTB2, 0, st>>>(d_tasks, d_items, d_segs);
-      else eval_kernel<FAM, MIXED, true><<<n_on, kTB, 0, st>>>(d_tasks, d_items, d_segs);
-    }
-    if (nitems > n_on)
-      eval_kernel<FAM, MIXED, false><<<nitems - n_on, kTB, 0, two ? side : st>>>(d_tasks, d_items + n_on, d_segs);
-    if (two) {
-      cudaEventRecord(join, side);
-      cudaStreamWaitEvent(st, join, 0);
-    }
-  } else {
-    eval_kernel<FAM, MIXED, false><<<nitems, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+  const bool two = n_on > 0 && nitems > n_on && side;
+  cudaStream_t s2 = two ? side : st;
+  if (two) {
+    cudaEventRecord(fork, st);
+    cudaStreamWaitEvent(side, fork, 0);
+  }
+  if (n_on > 0) {
+    if constexpr (MIXED && FAM != F_E2G) eval_kernel_on2<FAM><<<n_on, kTB2, 0, st>>>(d_tasks, d_items, d_segs);
+    else eval_kernel<FAM, MIXED, true><<<n_on, kTB, 0, st>>>(d_tasks, d_items, d_segs);
+  }
+  if (nitems > n_on) eval_kernel<FAM, MIXED, false><<<nitems - n_on, kTB, 0, s2>>>(d_tasks, d_items + n_on, d_segs);
+  if (two) {
+    cudaEventRecord(join, side);
+    cudaStreamWaitEvent(st, join, 0);
   }
 }
 
@@ -1236,11 +1232,11 @@ void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_items, c
     if (!mixed) {
       if (family == F_SL) launch_family<F_SL, false>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
       else if (family == F_DL) launch_family<F_DL, false>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
-      else launch_family<F_E2G, false>(d_tasks, d_items, d_segs, nitems, 0, st, side, fork, join);
+      else launch_family<F_E2G, false>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
     } else {
       if (family == F_SL) launch_family<F_SL, true>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
       else if (family == F_DL) launch_family<F_DL, true>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
-      else launch_family<F_E2G, true>(d_tasks, d_items, d_segs, nitems, 0, st, side, fork, join);
+      else launch_family<F_E2G, true>(d_tasks, d_items, d_segs, nitems, n_on, st, side, fork, join);
     }
   }
   if (ntask_blocks > 0) reduce_kernel<<<ntask_blocks, kTB, 0, st>>>(d_tasks, d_task_blocks);

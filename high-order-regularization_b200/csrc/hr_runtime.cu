@@ -282,10 +282,11 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
     }
     starts.push_back(slot);
   }
-  // on-surface items first (their own launch), each part by decreasing cost
+  // lean items first (their own launch: on-surface kinds, or the extend-to-grid
+  // box-face sums), each part by decreasing cost
   auto on_kind = [&](const BlockRef& r) {
     const int k = tasks[r.task].kind;
-    return family != F_E2G && (k == K_SL_ON || k == K_DL_ON);
+    return family == F_E2G ? (k == K_E2G_SL_AWAY || k == K_E2G_P_AWAY) : (k == K_SL_ON || k == K_DL_ON);
   };
   std::stable_sort(items.begin(), items.end(),
                    [&](const std::pair<double, BlockRef>& a, const std::pair<double, BlockRef>& b) {

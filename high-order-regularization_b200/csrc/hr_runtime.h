@@ -150,7 +150,7 @@ struct Batch {
   DBuf<int2> d_task_blocks;
   DBuf<double> d_partial;
   int nitems = 0, ntask_blocks = 0;
-  int n_on = 0;  // leading items of on-surface tasks (launched on their own)
+  int n_on = 0;  // leading lean items (on-surface / box-face tasks, launched on their own)
   bool ready = false;  // finalize has run
   // builds the segments and cost-balanced work items of all tasks
   void finalize(cudaStream_t st, int num_sms = 148);
