@@ -26,6 +26,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -56,8 +57,10 @@ class ClockSampler:
 
     def start(self):
         try:
-            os.makedirs(os.path.join(ROOT, "gpurun_out"), exist_ok=True)
-            self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % self.device)
+            # raw samples: HR_CLOCKS_DIR if set, else the system temporary directory
+            d = os.environ.get("HR_CLOCKS_DIR") or tempfile.gettempdir()
+            os.makedirs(d, exist_ok=True)
+            self.path = os.path.join(d, "clocks_bench_%d.csv" % self.device)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,

@@ -67,7 +67,7 @@ def _exact_grids(N, h):
 
 
 def test_exact_solution_error_table_h32(ctx):
-    """E2G N = 96: the reference's own error table (the survey's golden values)."""
+    """E2G N = 96: the reference's own error table (its printed golden values)."""
     e = highreg.E2G(ctx, 96)
     with pytest.raises(highreg.HrError):  # no slices before a run
         e.midplane()
