@@ -9,8 +9,9 @@
 // with M = (P+1)^2 <= 128 rows (padded to 128), N = C (P+1) columns (padded to
 // a multiple of 16) and K = the node's sources. One CTA of 128 threads per
 // work item (a node and up to 512 of its sources):
-//   * threads 0..31 evaluate the barycentric Lagrange values of a tile of 32
-//     sources (FP64, the reference's removable-singularity rule) and the
+//   * threads 0..95 evaluate the barycentric Lagrange values of a tile of 32
+//     sources, one (axis, source) each (offsets in FP64 for the reference's
+//     removable-singularity rule, quotients in FP32), threads 96..127 the
 //     channel values a_s q_c(s);
 //   * all threads form the A and B tiles in shared memory, K-major, in the
 //     no-swizzle canonical layout (8-row x 16-byte core matrices; K-chunk
@@ -41,6 +42,7 @@ namespace {
 
 constexpr int kTcThreads = 128;
 constexpr int kTcK = 32;          // sources per K tile
+static_assert(kTcThreads == 4 * kTcK, "three warps of Lagrange values and one of channel values per tile");
 constexpr int kTcMaxP1 = 11;      // (P+1)^2 <= 128
 constexpr long kWaitLimit = 1L << 26;
 
@@ -152,43 +154,51 @@ __global__ void __launch_bounds__(kTcThreads) moments_tc_kernel(
 
   for (int kt = 0; kt < ntile && ok; kt++) {
     const int s0 = it.s0 + kt * kTcK;
-    // Lagrange values of this tile's sources (overlaps the previous tile's MMAs)
-    if (tid < kTcK) {
-      const int s = s0 + tid;
+    // Lagrange values of this tile's sources (overlaps the previous tile's MMAs):
+    // threads 0..95 one (axis, source) each — the offset from each Chebyshev
+    // point in FP64 (for the reference's removable-singularity test), the
+    // barycentric quotients in FP32, which is all the TF32 split keeps —
+    // and threads 96..127 the channel values a_s q_c(s) of one source each
+    if (tid < 3 * kTcK) {
+      const int ax = tid / kTcK, src = tid - ax * kTcK;
+      const int s = s0 + src;
       const bool valid = s < it.s1;
-      const double px[3] = {valid ? x[s] : 0.0, valid ? y[s] : 0.0, valid ? z[s] : 0.0};
-      for (int ax = 0; ax < 3; ax++) {
-        double L[kTcMaxP1];
-        int flag = -1;
-        double S = 0.0;
-        for (int jj = 0; jj < P1; jj++) {
-          // w_j = (-1)^j d_j, d_0 = d_P = 1/2 (2S/KITC.cpp:365-375)
-          const double w = ((jj % 2 == 0) ? 1.0 : -1.0) * ((jj == 0 || jj == P1 - 1) ? 0.5 : 1.0);
-          const double d = px[ax] - sT[ax * P1 + jj];
-          if (fabs(d) < 1.e-07) {
-            flag = jj;
-            L[jj] = 0.0;
-          } else {
-            L[jj] = w / d;
-            S += L[jj];
-          }
-        }
-        for (int jj = 0; jj < P1; jj++) {
-          const double v = (flag > -1) ? (jj == flag ? 1.0 : 0.0) : L[jj] / S;
-          sL[(ax * kTcMaxP1 + jj) * kTcK + tid] = valid ? (float)v : 0.f;
+      const double pc = valid ? (ax == 0 ? x[s] : (ax == 1 ? y[s] : z[s])) : 0.0;
+      float L[kTcMaxP1];
+      int flag = -1;
+      float S = 0.f;
+      for (int jj = 0; jj < P1; jj++) {
+        // w_j = (-1)^j d_j, d_0 = d_P = 1/2 (2S/KITC.cpp:365-375)
+        const float w = ((jj % 2 == 0) ? 1.f : -1.f) * ((jj == 0 || jj == P1 - 1) ? 0.5f : 1.f);
+        const double d = pc - sT[ax * P1 + jj];
+        if (fabs(d) < 1.e-07) {
+          flag = jj;
+          L[jj] = 0.f;
+        } else {
+          L[jj] = w / (float)d;
+          S += L[jj];
         }
       }
+      const float inv = 1.f / S;
+      for (int jj = 0; jj < P1; jj++) {
+        const float v = (flag > -1) ? (jj == flag ? 1.f : 0.f) : L[jj] * inv;
+        sL[(ax * kTcMaxP1 + jj) * kTcK + src] = valid ? v : 0.f;
+      }
+    } else {
+      const int src = tid - 3 * kTcK;
+      const int s = s0 + src;
+      const bool valid = s < it.s1;
       const double as = valid ? a[s] : 0.0;
       const double n3[3] = {valid ? nx[s] : 0.0, valid ? ny[s] : 0.0, valid ? nz[s] : 0.0};
       const double q3[3] = {valid ? qx[s] : 0.0, valid ? qy[s] : 0.0, valid ? qz[s] : 0.0};
       if (DL) {
         for (int l = 0; l < 3; l++)
-          for (int m = 0; m < 3; m++) sAQ[(3 * l + m) * kTcK + tid] = (float)(as * q3[l] * n3[m]);
-        for (int m = 0; m < 3; m++) sAQ[(9 + m) * kTcK + tid] = (float)(as * n3[m]);
+          for (int m = 0; m < 3; m++) sAQ[(3 * l + m) * kTcK + src] = (float)(as * q3[l] * n3[m]);
+        for (int m = 0; m < 3; m++) sAQ[(9 + m) * kTcK + src] = (float)(as * n3[m]);
       } else {
         for (int m = 0; m < 3; m++) {
-          sAQ[m * kTcK + tid] = (float)(as * q3[m]);
-          sAQ[(3 + m) * kTcK + tid] = (float)(as * n3[m]);
+          sAQ[m * kTcK + src] = (float)(as * q3[m]);
+          sAQ[(3 + m) * kTcK + src] = (float)(as * n3[m]);
         }
       }
     }
