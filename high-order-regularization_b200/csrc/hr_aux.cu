@@ -9,6 +9,7 @@ namespace {
 
 constexpr int kMomThreads = 384;
 constexpr int kMomTile = 64;  // sources staged per sub-tile
+static_assert(kMomThreads >= 4 * kMomTile, "a thread per (axis, source) and per source for the channels");
 constexpr int kMaxP1 = 16;
 
 // Upward pass of one (node, source range) item: the barycentric Lagrange
@@ -25,8 +26,7 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(
     const double* __restrict__ a, const double* __restrict__ qx, const double* __restrict__ qy,
     const double* __restrict__ qz, double* __restrict__ partial) {
   constexpr int C = DL ? 12 : 6;
-  __shared__ double sL[3][kMaxP1][kMomTile];  // Lagrange numerators per axis
-  __shared__ double sD[kMomTile];             // 1 / (S1 S2 S3)
+  __shared__ double sL[3][kMaxP1][kMomTile];  // normalized Lagrange values per axis
   __shared__ double sA[kMomTile];
   __shared__ double sQ[C][kMomTile];
   __shared__ double sT[3 * kMaxP1];
@@ -45,51 +45,55 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(
     for (int s0 = it.s0; s0 < it.s1; s0 += kMomTile) {
       const int cnt = min(kMomTile, it.s1 - s0);
       __syncthreads();
-      if (tid < cnt) {
-        const int s = s0 + tid;
-        const double px[3] = {x[s], y[s], z[s]};
-        double D = 1.0;
-        for (int ax = 0; ax < 3; ax++) {
+      // threads 0..191: the Lagrange values of one (axis, source) each,
+      // normalized by their own axis sum; threads 192..255: area and channel
+      // values of one source each
+      if (tid < 3 * kMomTile) {
+        const int ax = tid / kMomTile, src = tid - ax * kMomTile;
+        if (src < cnt) {
+          const int s = s0 + src;
+          const double pc = ax == 0 ? x[s] : (ax == 1 ? y[s] : z[s]);
+          double L[kMaxP1];
           int flag = -1;
           double S = 0.0;
           for (int jj = 0; jj < P1; jj++) {
-            double w = ((jj % 2 == 0) ? 1.0 : -1.0) * ((jj == 0 || jj == P1 - 1) ? 0.5 : 1.0);
-            double d = px[ax] - sT[ax * P1 + jj];
+            const double w = ((jj % 2 == 0) ? 1.0 : -1.0) * ((jj == 0 || jj == P1 - 1) ? 0.5 : 1.0);
+            const double d = pc - sT[ax * P1 + jj];
             if (fabs(d) < 1.e-07) {
               flag = jj;
-              sL[ax][jj][tid] = 0.0;
+              L[jj] = 0.0;
             } else {
-              double tt = w / d;
-              sL[ax][jj][tid] = tt;
-              S += tt;
+              L[jj] = w / d;
+              S += L[jj];
             }
           }
-          if (flag > -1) {
-            S = 1.0;
-            for (int jj = 0; jj < P1; jj++) sL[ax][jj][tid] = (jj == flag) ? 1.0 : 0.0;
-          }
-          D = (ax == 0) ? S : D * S;
+          const double inv = 1.0 / S;
+          for (int jj = 0; jj < P1; jj++)
+            sL[ax][jj][src] = (flag > -1) ? (jj == flag ? 1.0 : 0.0) : L[jj] * inv;
         }
-        sD[tid] = 1.0 / D;
-        sA[tid] = a[s];
-        const double n3[3] = {nx[s], ny[s], nz[s]};
-        const double q3[3] = {qx[s], qy[s], qz[s]};
-        if (DL) {
-          for (int l = 0; l < 3; l++)
-            for (int m = 0; m < 3; m++) sQ[3 * l + m][tid] = q3[l] * n3[m];
-          for (int m = 0; m < 3; m++) sQ[9 + m][tid] = n3[m];
-        } else {
-          for (int m = 0; m < 3; m++) {
-            sQ[m][tid] = q3[m];
-            sQ[3 + m][tid] = n3[m];
+      } else if (tid < 4 * kMomTile) {
+        const int src = tid - 3 * kMomTile;
+        if (src < cnt) {
+          const int s = s0 + src;
+          sA[src] = a[s];
+          const double n3[3] = {nx[s], ny[s], nz[s]};
+          const double q3[3] = {qx[s], qy[s], qz[s]};
+          if (DL) {
+            for (int l = 0; l < 3; l++)
+              for (int m = 0; m < 3; m++) sQ[3 * l + m][src] = q3[l] * n3[m];
+            for (int m = 0; m < 3; m++) sQ[9 + m][src] = n3[m];
+          } else {
+            for (int m = 0; m < 3; m++) {
+              sQ[m][src] = q3[m];
+              sQ[3 + m][src] = n3[m];
+            }
           }
         }
       }
       __syncthreads();
       if (kk < Pf) {
         for (int s = 0; s < cnt; s++) {
-          double v = sL[0][i][s] * sL[1][j][s] * sL[2][k][s] * sD[s];
-          v *= sA[s];
+          const double v = sL[0][i][s] * sL[1][j][s] * sL[2][k][s] * sA[s];
 #pragma unroll
           for (int c = 0; c < C; c++) acc[c] += v * sQ[c][s];
         }
