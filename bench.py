@@ -371,22 +371,28 @@ def run_ours(args, rank, world, local_rank):
 
     # end to end through the C ABI with host buffers: scene upload + plan
     # (trees, interaction lists, stencils) + RHS + solve + solution read back
-    e2e_times, plan_times = [], []
+    e2e_times, plan_times, dev_times = [], [], []
     h2d = sum(np.asarray(v).nbytes for k, v in geo.items() if isinstance(v, np.ndarray))
-    for _ in range(max(1, min(args.steps, 5 if H_INV <= 64 else 3))):
+    n_e2e = max(1, min(args.steps, 5 if H_INV <= 64 else 3))
+    for k_e2e in range(n_e2e + 1):  # the first pass warms the host-buffer path and is not timed
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         p2 = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=P, N0=N0, theta=THETA)
         t1 = time.perf_counter()
         bh = p2.rhs(geo["f0"], geo["f1"])
         xh, r2 = p2.solve(bh, restart=RESTART, tol=TOL)
-        e2e_times.append(time.perf_counter() - t0)
-        plan_times.append(t1 - t0)
+        t2 = time.perf_counter()
         p2.close()
+        if k_e2e > 0:
+            e2e_times.append(t2 - t0)
+            plan_times.append(t1 - t0)
+            dev_times.append(r2["seconds"])
     e2e_t = max_over_ranks(statistics.median(e2e_times), world)
     e2e = {"value": sum_over_ranks(pairs_step, world) / e2e_t, "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(8 * n), "seconds_per_step": e2e_t,
+           "samples_seconds": [round(t, 4) for t in e2e_times],
            "plan_seconds": statistics.median(plan_times),
+           "solve_device_seconds": statistics.median(dev_times),
            "note": "scene upload and plan (trees, interaction lists, stencils on the host) + RHS + solve + "
                    "solution read back, through the C ABI with host buffers"}
 

@@ -5,7 +5,9 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <exception>
 #include <random>
+#include <thread>
 #include <vector>
 
 #include "hr_runtime.h"
@@ -455,6 +457,31 @@ struct hr_plan2s {
 
 namespace {
 
+// Runs a() on a second host thread (with `device` current there) and b() on
+// this one; rethrows the exception of either (b's first).
+template <class A, class B>
+void run_both(int device, A&& a, B&& b) {
+  std::exception_ptr ea, eb;
+  std::thread th([&] {
+    try {
+      HR_CHECK_CUDA(cudaSetDevice(device));
+      a();
+    } catch (...) {
+      ea = std::current_exception();
+    }
+  });
+  try {
+    b();
+  } catch (...) {
+    eb = std::current_exception();
+  }
+  th.join();
+  if (eb) std::rethrow_exception(eb);
+  if (ea) std::rethrow_exception(ea);
+}
+
+void sl_batch(hr_plan2s& P);
+
 // Stresslet batches of the matvec, one per precision in [prec0, prec1), over
 // the given trees and lists (the plan's own, or the inner operator's).
 void dl_batches(hr_plan2s& P, DevTree* tree, DevLists* Lon, DevLists* Loff, Batch* dl, int prec0, int prec1,
@@ -494,8 +521,13 @@ void plan_batches(hr_plan2s& P) {
   cudaStream_t st = P.C->stream;
   P.counters.alloc(4 * 8);
   P.counters.zero(st);
-  // the reduced-precision batches are built on first use (plan_matvec)
-  dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, 1, true);
+  // the reduced-precision batches are built on first use (plan_matvec); the
+  // FP64 stresslet and the Stokeslet batches are built on two host threads
+  run_both(P.C->device, [&] { dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, 1, true); }, [&] { sl_batch(P); });
+}
+
+void sl_batch(hr_plan2s& P) {
+  cudaStream_t st = P.C->stream;
   Batch& B = P.sl;
   B.family = F_SL;
   for (int t = 0; t < 2; t++) {
@@ -814,8 +846,11 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
     P->off[1] = 3 * P->nq[0];
     P->n = 3 * (P->nq[0] + P->nq[1]);
     const bool direct = opt->mode == HR_DIRECT;
-    for (int s = 0; s < 2; s++) P->tree[s].build(sc->surf[s], opt->P, opt->N0, opt->theta, direct, st);
-    for (int t = 0; t < 2; t++) {
+    // the two surfaces' host planning runs on two host threads
+    run_both(
+        ctx->c.device, [&] { P->tree[1].build(sc->surf[1], opt->P, opt->N0, opt->theta, direct, st); },
+        [&] { P->tree[0].build(sc->surf[0], opt->P, opt->N0, opt->theta, direct, st); });
+    auto per_target_set = [&](int t) {
       const hr_targets& T = sc->tgt[t];
       std::vector<uint8_t> near = near_flags(T.n, T.b, sc->delta);
       P->near_host[t] = near;
@@ -830,7 +865,8 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
       P->sten[t].build(s, st);
       P->out_on[t].alloc(3 * (size_t)T.n);
       P->out_off[t].alloc(3 * (size_t)T.n);
-    }
+    };
+    run_both(ctx->c.device, [&] { per_target_set(1); }, [&] { per_target_set(0); });
     P->xin.alloc(P->n);
     P->fin.alloc(P->n);
     P->r.alloc(P->n);
