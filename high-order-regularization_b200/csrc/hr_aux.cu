@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(
 }
 
 // Sums the partial moments of each node in item order (deterministic) and
-// stores them proxy-major, one thread per proxy. The stresslet's 12 channels
+// stores them proxy-major. The stresslet's 12 channels
 // (g (x) n, g-major, then n) enter the far field only through
 //   d.M.d = M00 d0^2 + M11 d1^2 + M22 d2^2 + (M01 + M10) d0 d1
 //         + (M02 + M20) d0 d2 + (M12 + M21) d1 d2   and   Mn.d,
@@ -118,30 +118,36 @@ __global__ void __launch_bounds__(kMomThreads) moments_kernel(
 __global__ void moments_reduce_kernel(int C, int Pf, const int* __restrict__ item_start,
                                       const double* __restrict__ partial, double* __restrict__ mom,
                                       float* __restrict__ momf) {
-  const int node = blockIdx.y;
+  // one thread per (node, proxy, stored value): a value is one channel, or for
+  // the stresslet's symmetric combinations the sum of two, each summed over
+  // the node's items in item order
+  const int node = blockIdx.y, o = blockIdx.z;
   const int kk = blockIdx.x * blockDim.x + threadIdx.x;
   if (kk >= Pf) return;
-  const int a = item_start[node], b = item_start[node + 1];
-  double m[12];
-#pragma unroll
-  for (int c = 0; c < 12; c++) m[c] = 0.0;
-  for (int q = a; q < b; q++) {
-#pragma unroll
-    for (int c = 0; c < 12; c++)
-      if (c < C) m[c] += partial[((size_t)q * C + c) * Pf + kk];
+  const bool dl = C == 12;
+  int c0 = o, c1 = -1;
+  if (dl) {
+    const int first[10] = {0, 4, 8, 1, 2, 5, 9, 10, 11, -1};
+    const int second[10] = {-1, -1, -1, 3, 6, 7, -1, -1, -1, -1};
+    c0 = first[o];
+    c1 = second[o];
   }
+  const int a = item_start[node], b = item_start[node + 1];
+  double s0 = 0.0, s1 = 0.0;
+  if (c0 >= 0)
+    for (int q = a; q < b; q++) s0 += partial[((size_t)q * C + c0) * Pf + kk];
+  if (c1 >= 0)
+    for (int q = a; q < b; q++) s1 += partial[((size_t)q * C + c1) * Pf + kk];
+  const double v = c1 >= 0 ? s0 + s1 : s0;
   const size_t k = (size_t)node * Pf + kk;
-  if (C == 12) {
-    const double o[10] = {m[0], m[4], m[8], m[1] + m[3], m[2] + m[6], m[5] + m[7], m[9], m[10], m[11], 0.0};
-#pragma unroll
-    for (int i = 0; i < 10; i++) mom[k * 10 + i] = o[i];
-#pragma unroll
-    for (int i = 0; i < 12; i++) momf[k * 12 + i] = i < 9 ? (float)o[i] : 0.f;
+  if (dl) {
+    mom[k * 10 + o] = v;  // o = 9: the zero pad
+    momf[k * 12 + o] = (float)v;
+    if (o == 9) momf[k * 12 + 10] = momf[k * 12 + 11] = 0.f;
   } else {
-#pragma unroll
-    for (int i = 0; i < 6; i++) mom[k * 6 + i] = m[i];
-#pragma unroll
-    for (int i = 0; i < 8; i++) momf[k * 8 + i] = i < 6 ? (float)m[i] : 0.f;
+    mom[k * 6 + o] = v;
+    momf[k * 8 + o] = (float)v;
+    if (o == 5) momf[k * 8 + 6] = momf[k * 8 + 7] = 0.f;
   }
 }
 
@@ -345,7 +351,7 @@ void launch_moments(int dl, const MomItem* d_items, int nitems, int P1, const do
 void launch_moments_reduce(int C, int Pf, int nnodes_out, const int* d_item_start,
                            const double* partial, double* mom, float* momf, cudaStream_t st) {
   if (nnodes_out <= 0) return;
-  dim3 grid((Pf + 127) / 128, nnodes_out);
+  dim3 grid((Pf + 127) / 128, nnodes_out, C == 12 ? 10 : 6);
   moments_reduce_kernel<<<grid, 128, 0, st>>>(C, Pf, d_item_start, partial, mom, momf);
 }
 
