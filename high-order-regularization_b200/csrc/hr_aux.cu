@@ -264,13 +264,16 @@ __global__ void __launch_bounds__(kDotThreads) dots_kernel(int n, int ncols,
   }
 }
 
+// One warp per column: lane l sums blocks l, l + 32, ... in order, then a
+// fixed shuffle tree adds the lanes (deterministic).
 __global__ void dots_finalize_kernel(int ncols, int nblk, const double* __restrict__ partial,
                                      double* __restrict__ out) {
-  const int c = threadIdx.x;
+  const int c = blockIdx.x, lane = threadIdx.x;
   if (c >= ncols) return;
   double s = 0.0;
-  for (int b = 0; b < nblk; b++) s += partial[(size_t)b * kMaxCols + c];
-  out[c] = s;
+  for (int b = lane; b < nblk; b += 32) s += partial[(size_t)b * kMaxCols + c];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+  if (lane == 0) out[c] = s;
 }
 
 // w += sign * sum_c coef[c] V[c]
@@ -390,7 +393,7 @@ void launch_dots(int n, int ncols, const double* V, long ldv, const double* w, d
 }
 
 void launch_dots_finalize(int ncols, const double* partial, double* out, cudaStream_t st) {
-  dots_finalize_kernel<<<1, kMaxCols, 0, st>>>(ncols, kRedBlocks, partial, out);
+  dots_finalize_kernel<<<ncols, 32, 0, st>>>(ncols, kRedBlocks, partial, out);
 }
 
 void launch_axpy_multi(int n, int ncols, const double* V, long ldv, const double* coef,

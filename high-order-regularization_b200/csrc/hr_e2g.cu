@@ -234,6 +234,26 @@ struct hr_e2g {
   ~hr_e2g() { poisson_work_destroy(pw); }
 };
 
+// The four sums of one run in one batch, in precision prec.
+static void e2g_batch(hr_e2g& E, int prec, Ctx& C) {
+  const double p_scale = 1.0 / (4.0 * kPI), sl_scale = 1.0 / (8.0 * kPI);
+  const double delta = E.S.delta;
+  Batch& B = E.batch[prec];
+  B.family = F_E2G;
+  EvalTask a = make_task(K_E2G_P_AWAY, delta, p_scale, E.tree, E.Lf, E.tf, E.pf.p);
+  EvalTask b = make_task(K_E2G_SL_AWAY, delta, sl_scale, E.tree, E.Lf, E.tf, E.uf.p);
+  EvalTask c = make_task(K_E2G_P7, delta, -p_scale, E.tree, E.Lb, E.tb, E.pb.p);
+  EvalTask d = make_task(K_E2G_SL7, delta, sl_scale, E.tree, E.Lb, E.tb, E.ub.p);
+  for (EvalTask* t : {&a, &b, &c, &d}) {
+    t->mixed = prec;
+    t->jump_mode = 1;
+  }
+  B.tasks = {a, b, c, d};
+  B.lists = {&E.Lf.host, &E.Lf.host, &E.Lb.host, &E.Lb.host};
+  B.trees = {&E.tree.host, &E.tree.host, &E.tree.host, &E.tree.host};
+  B.finalize(C.stream, C.num_sms);
+}
+
 extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
   if (!ctx || !out || N < 36 || N % 2 != 0) return HR_ERR_ARG;
   *out = nullptr;
@@ -324,23 +344,7 @@ extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
     E->uf.alloc(3 * (size_t)E->nface);
     E->pb.alloc(std::max(1, E->nband));
     E->ub.alloc(3 * (size_t)std::max(1, E->nband));
-    const double p_scale = 1.0 / (4.0 * kPI), sl_scale = 1.0 / (8.0 * kPI);
-    for (int prec = 0; prec < 3; prec++) {
-      Batch& B = E->batch[prec];
-      B.family = F_E2G;
-      EvalTask a = make_task(K_E2G_P_AWAY, S.delta, p_scale, E->tree, E->Lf, E->tf, E->pf.p);
-      EvalTask b = make_task(K_E2G_SL_AWAY, S.delta, sl_scale, E->tree, E->Lf, E->tf, E->uf.p);
-      EvalTask c = make_task(K_E2G_P7, S.delta, -p_scale, E->tree, E->Lb, E->tb, E->pb.p);
-      EvalTask d = make_task(K_E2G_SL7, S.delta, sl_scale, E->tree, E->Lb, E->tb, E->ub.p);
-      for (EvalTask* t : {&a, &b, &c, &d}) {
-        t->mixed = prec;
-        t->jump_mode = 1;
-      }
-      B.tasks = {a, b, c, d};
-      B.lists = {&E->Lf.host, &E->Lf.host, &E->Lb.host, &E->Lb.host};
-      B.trees = {&E->tree.host, &E->tree.host, &E->tree.host, &E->tree.host};
-      B.finalize(st, C.num_sms);
-    }
+    e2g_batch(*E, HR_FP64, C);  // the reduced-precision batches are built on first use
     E->pairs = 2LL * (E->nface + E->nband) * (long long)surf.n;
     // masks: BAND2 points, and exterior points outside BAND2 (E2G/main.cpp:1611-1614, 1654-1672)
     std::vector<uint8_t> b2((size_t)M * M * M, 0), om((size_t)M * M * M, 0);
@@ -396,10 +400,11 @@ extern "C" int hr_e2g_run(hr_e2g* E, int precision, hr_e2g_report* rep) {
     cudaStream_t st = C.stream;
     const int N = E->S.N, M = N + 1;
     const long m3 = (long)M * M * M;
+    HR_REQUIRE(precision == HR_FP64 || precision == HR_MIXED || precision == HR_FP32, "unknown precision");
+    if (!E->batch[precision].ready) e2g_batch(*E, precision, C);  // before the timed region
     cudaEvent_t ev[4];
     for (auto& e : ev) HR_CHECK_CUDA(cudaEventCreate(&e));
     HR_CHECK_CUDA(cudaEventRecord(ev[0], st));
-    HR_REQUIRE(precision == HR_FP64 || precision == HR_MIXED || precision == HR_FP32, "unknown precision");
     E->batch[precision].launch(C);
     E->ran = true;
     HR_CHECK_CUDA(cudaEventRecord(ev[1], st));
