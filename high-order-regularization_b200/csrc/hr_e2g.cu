@@ -282,34 +282,55 @@ extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
     std::vector<double> fx;
     std::vector<long> fg;
     for (int i = 0; i <= N; i++)
-      for (int j = 0; j <= N; j++)
-        for (int k = 0; k <= N; k++)
-          if (i == 0 || i == N || j == 0 || j == N || k == 0 || k == N) {
-            fx.insert(fx.end(), {i * h, j * h, k * h});
-            fg.push_back(((long)i * M + j) * M + k);
-          }
+      for (int j = 0; j <= N; j++) {
+        // an (i, j) column off the box's i and j faces meets the box only at k = 0 and k = N
+        const bool all = (i == 0 || i == N || j == 0 || j == N);
+        for (int k = 0; k <= N; k += (all || k == N) ? 1 : N) {
+          fx.insert(fx.end(), {i * h, j * h, k * h});
+          fg.push_back(((long)i * M + j) * M + k);
+        }
+      }
     // band targets outside or on the surface (E2G/main.cpp:1133-1162)
+    // (one i-slab per OpenMP iteration, slabs concatenated in i order)
     std::vector<double> bx, bb, bx0, bn0, bf0;
     std::vector<long> bg;
-    for (int i = 1; i < N; i++)
-      for (int j = 1; j < N; j++)
-        for (int k = 1; k < N; k++) {
-          long g = ((long)i * M + j) * M + k;
-          int ind = S.nrst[g];
-          if (ind == -1) continue;
-          double b = S.b[ind];
-          if ((b > 0.0) || (fabs(b) < 1.e-12)) {
-            bx.insert(bx.end(), {i * h, j * h, k * h});
-            bb.push_back(b);
-            const double* x0 = &S.x0[3 * ind];
-            bx0.insert(bx0.end(), {x0[0], x0[1], x0[2]});
-            bn0.insert(bn0.end(), {S.n0[3 * ind], S.n0[3 * ind + 1], S.n0[3 * ind + 2]});
-            double f0[3];
-            e2g_setup::stokeslet_density(x0, f0);
-            bf0.insert(bf0.end(), {f0[0], f0[1], f0[2]});
-            bg.push_back(g);
+    {
+      struct Slab {
+        std::vector<double> x, b, x0, n0, f0;
+        std::vector<long> g;
+      };
+      std::vector<Slab> slab(N + 1);
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int i = 1; i < N; i++) {
+        Slab& L = slab[i];
+        for (int j = 1; j < N; j++)
+          for (int k = 1; k < N; k++) {
+            long g = ((long)i * M + j) * M + k;
+            int ind = S.nrst[g];
+            if (ind == -1) continue;
+            double b = S.b[ind];
+            if ((b > 0.0) || (fabs(b) < 1.e-12)) {
+              L.x.insert(L.x.end(), {i * h, j * h, k * h});
+              L.b.push_back(b);
+              const double* x0 = &S.x0[3 * ind];
+              L.x0.insert(L.x0.end(), {x0[0], x0[1], x0[2]});
+              L.n0.insert(L.n0.end(), {S.n0[3 * ind], S.n0[3 * ind + 1], S.n0[3 * ind + 2]});
+              double f0[3];
+              e2g_setup::stokeslet_density(x0, f0);
+              L.f0.insert(L.f0.end(), {f0[0], f0[1], f0[2]});
+              L.g.push_back(g);
+            }
           }
-        }
+      }
+      for (const Slab& L : slab) {
+        bx.insert(bx.end(), L.x.begin(), L.x.end());
+        bb.insert(bb.end(), L.b.begin(), L.b.end());
+        bx0.insert(bx0.end(), L.x0.begin(), L.x0.end());
+        bn0.insert(bn0.end(), L.n0.begin(), L.n0.end());
+        bf0.insert(bf0.end(), L.f0.begin(), L.f0.end());
+        bg.insert(bg.end(), L.g.begin(), L.g.end());
+      }
+    }
     E->nface = (int)fg.size();
     E->nband = (int)bg.size();
     auto up = [&](DevTargets& T, int n, const std::vector<double>& x, const double* b,
@@ -348,6 +369,7 @@ extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
     E->pairs = 2LL * (E->nface + E->nband) * (long long)surf.n;
     // masks: BAND2 points, and exterior points outside BAND2 (E2G/main.cpp:1611-1614, 1654-1672)
     std::vector<uint8_t> b2((size_t)M * M * M, 0), om((size_t)M * M * M, 0);
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < M; i++)
       for (int j = 0; j < M; j++)
         for (int k = 0; k < M; k++) {
