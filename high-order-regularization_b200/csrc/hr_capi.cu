@@ -10,6 +10,8 @@
 #include <thread>
 #include <vector>
 
+#include <omp.h>
+
 #include "hr_runtime.h"
 
 using namespace hr;
@@ -458,23 +460,30 @@ struct hr_plan2s {
 namespace {
 
 // Runs a() on a second host thread (with `device` current there) and b() on
-// this one; rethrows the exception of either (b's first).
+// this one, each with half of the host's cores for its OpenMP loops (so the
+// two teams do not oversubscribe them); rethrows the exception of either
+// (b's first).
 template <class A, class B>
 void run_both(int device, A&& a, B&& b) {
+  const int half = std::max(1, omp_get_num_procs() / 2);
+  const int before = omp_get_max_threads();
   std::exception_ptr ea, eb;
   std::thread th([&] {
     try {
+      omp_set_num_threads(half);
       HR_CHECK_CUDA(cudaSetDevice(device));
       a();
     } catch (...) {
       ea = std::current_exception();
     }
   });
+  omp_set_num_threads(half);
   try {
     b();
   } catch (...) {
     eb = std::current_exception();
   }
+  omp_set_num_threads(before);
   th.join();
   if (eb) std::rethrow_exception(eb);
   if (ea) std::rethrow_exception(ea);

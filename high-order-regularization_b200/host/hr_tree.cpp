@@ -240,13 +240,16 @@ Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near
     std::vector<int> slot(2 * (size_t)nn, -1);
     std::vector<int> touched;
     std::vector<int> stack;
+    std::vector<std::vector<int>> keys(kTB);  // each target's entries, in traversal order
+    std::vector<int> order(kTB), tsave(kTB);
 #pragma omp for schedule(dynamic, 4)
     for (int b = 0; b < nb; b++) {
       std::vector<Entry>& E = per[b];
       touched.clear();
-      for (int tt = 0; tt < kTB; tt++) {
+      const int cnt_t = std::min(kTB, nt - b * kTB);
+      for (int tt = 0; tt < cnt_t; tt++) {
+        keys[tt].clear();
         int k = b * kTB + tt;
-        if (k >= nt) break;
         int t = L.tord[k];
         const double px = txyz[3 * t], py = txyz[3 * t + 1], pz = txyz[3 * t + 2];
         bool regt = near ? near[t] != 0 : true;
@@ -272,17 +275,31 @@ Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near
               stack.push_back(T.children[T.child_start[c] + q]);
             continue;
           }
-          int key = 2 * c + type;
+          keys[tt].push_back(2 * c + type);
+        }
+      }
+      // Targets with the same (or a similar) interaction list take neighbouring
+      // positions, so that a warp's 32 targets tend to share their entries and
+      // warps skip more entries whole. A target's sums do not depend on its
+      // position in the block.
+      for (int tt = 0; tt < cnt_t; tt++) order[tt] = tt;
+      std::stable_sort(order.begin(), order.begin() + cnt_t,
+                       [&](int x, int y) { return keys[x] < keys[y]; });
+      for (int tt = 0; tt < cnt_t; tt++) tsave[tt] = L.tord[b * kTB + tt];
+      for (int pos = 0; pos < cnt_t; pos++) {
+        const int tt = order[pos];
+        L.tord[b * kTB + pos] = tsave[tt];
+        for (int key : keys[tt]) {
           if (slot[key] < 0) {
             slot[key] = (int)E.size();
             touched.push_back(key);
             Entry e;
-            e.node = c;
-            e.type = type;
+            e.node = key >> 1;
+            e.type = key & 1;
             e.mask[0] = e.mask[1] = e.mask[2] = e.mask[3] = 0u;
             E.push_back(e);
           }
-          E[slot[key]].mask[tt >> 5] |= 1u << (tt & 31);
+          E[slot[key]].mask[pos >> 5] |= 1u << (pos & 31);
         }
       }
       for (int key : touched) slot[key] = -1;
