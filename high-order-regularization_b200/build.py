@@ -60,7 +60,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
             cmd = ["g++"] + CXXFLAGS + ["-c", src, "-o", obj]
         logs.append(_run(cmd, verbose))
     if force or not os.path.exists(LIB) or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcufft", "-Xcompiler", "-fopenmp", "-lgomp"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-Xcompiler", "-fopenmp", "-lgomp"]
         logs.append(_run(cmd, verbose))
     # the reference-signature layer, a separate library over the C ABI
     src = os.path.join(HERE, "host", "hr_ref_api.cpp")

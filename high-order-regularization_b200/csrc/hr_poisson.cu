@@ -1,21 +1,30 @@
 // hr_poisson.cu — the extend-to-grid Poisson solve on the device
 // (solve_Poisson + fftw_DST_Poisson3d_FD, E2G/main.cpp:969-1044, 1423-1823).
 //
-// DST-I (FFTW RODFT00, unnormalised) of length n along one axis is computed
-// from a real FFT of length N = n + 1 with the classical sine-transform
-// pre/post-processing (the auxiliary-array method for the sine transform,
-// e.g. Press et al., Numerical Recipes, "sinft"):
-//   y_0 = 0,  y_j = sin(j pi/N) (x_j + x_{N-j}) + (x_j - x_{N-j}) / 2,
-//   Y_k = sum_j y_j e^{-2 pi i jk/N} = R_k + i I_k,
-//   F_{2k} = -I_k,  F_1 = R_0 / 2,  F_{2k+1} = F_{2k-1} + R_k,
-// where F_k = sum_j x_j sin(pi jk/N) and RODFT00 returns 2 F_{k}, k = 1..n.
-// Each pass transforms along the contiguous axis and its post kernel writes
-// the result with the axes rotated ([a][b][c] -> [c][a][b]), so three passes
-// cover the three axes and restore the layout. The last forward pass divides
-// by the eigenvalues of the 4th-order compact Laplacian; the last inverse
-// pass applies the 1/(2(n+1))^3 scale and adds the extension w into u.
-#include <cufft.h>
-
+// The 3D DST-I (FFTW RODFT00, unnormalised) is three passes of one fused
+// kernel. A pass transforms the n-point lines along the contiguous axis and
+// writes its result with the axes rotated ([a][b][c] -> [c][a][b]), so three
+// passes cover the three axes and restore the layout. Each CTA takes
+// kDstLines consecutive lines (one contiguous span of the grid) and, in
+// shared memory:
+//   1. forms the length-N = n + 1 real sequence of the sine-transform
+//      auxiliary-array method (Press et al., Numerical Recipes, "sinft"):
+//        y_0 = 0,  y_j = sin(j pi/N) (x_j + x_{N-j}) + (x_j - x_{N-j}) / 2;
+//   2. packs it as P = N/2 complex values z_m = y_{2m} + i y_{2m+1} and runs a
+//      mixed-radix Stockham autosort FFT of length P (radix 8, 4, 2 and 3
+//      stages in registers, any other prime factor as a direct DFT stage);
+//   3. splits the result into the spectrum of the real sequence,
+//        Y_k = (Z_k + conj Z_{P-k})/2 - (i/2) e^{-2 pi i k/N} (Z_k - conj Z_{P-k}),
+//      and forms RODFT00's outputs 2F_1..2F_n from Y_k = R_k + i I_k:
+//        2F_1 = R_0,  2F_{2k} = -2 I_k,  2F_{2k+1} = 2F_{2k-1} + 2 R_k,
+//      the last recurrence as a warp prefix sum over k;
+//   4. writes each line's n outputs rotated, kDstLines consecutive doubles
+//      per output index, fused with the pass's epilogue.
+// A pass reads and writes the grid once. A Poisson solve is six passes
+// alternating between the data and one scratch grid: the third divides by the
+// eigenvalues of the 4th-order compact Laplacian, the sixth applies the
+// 1/(2(n+1))^3 scale and, for the extension, adds w into the interior of u.
+#include <algorithm>
 #include <cmath>
 #include <memory>
 #include <vector>
@@ -26,178 +35,463 @@ namespace hr {
 
 namespace {
 
-#define HR_CHECK_CUFFT(call)                                                       \
-  do {                                                                             \
-    cufftResult r_ = (call);                                                       \
-    if (r_ != CUFFT_SUCCESS)                                                       \
-      throw ::hr::Error(HR_ERR_CUDA, std::string(#call) + ": cufft error " + std::to_string((int)r_)); \
-  } while (0)
+constexpr int kDstLines = 8;      // lines per CTA (consecutive doubles per rotated store)
+constexpr int kDstThreads = 256;  // eight warps: one line per warp in the split step
+constexpr int kDstMaxStages = 24;
 
-// y[l][j] = sin(j pi/N)(x_j + x_{N-j}) + (x_j - x_{N-j})/2, x_j = in[l][j-1]
-__global__ void dst_pre_kernel(long lines, int n, const double* __restrict__ in,
-                               const double* __restrict__ sintab, double* __restrict__ y) {
-  const int N = n + 1;
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  long total = lines * N;
-  for (; idx < total; idx += (long)gridDim.x * blockDim.x) {
-    long l = idx / N;
-    int j = (int)(idx - l * N);
-    double v = 0.0;
-    if (j > 0) {
-      const double* row = in + l * n;
-      double xj = row[j - 1];
-      double xm = (N - j - 1 < n && N - j - 1 >= 0 && N - j != N) ? row[N - j - 1] : 0.0;
-      v = sintab[j] * (xj + xm) + 0.5 * (xj - xm);
+// Radices of the length-P complex FFT, in stage order.
+struct DstRadix {
+  int nst;
+  int r[kDstMaxStages];
+};
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cmul_mi(double2 a) { return make_double2(a.y, -a.x); }  // -i a
+
+// Forward DFTs (kernel e^{-2 pi i jk/R}) of 2, 3, 4 and 8 points in registers.
+__device__ __forceinline__ void dft2(double2& a, double2& b) {
+  const double2 t = a;
+  a = cadd(t, b);
+  b = csub(t, b);
+}
+
+__device__ __forceinline__ void dft3(double2& a, double2& b, double2& c) {
+  const double s = 0.86602540378443864676;  // sin(2 pi / 3)
+  const double2 t1 = cadd(b, c), t2 = csub(b, c);
+  const double2 m = make_double2(a.x - 0.5 * t1.x, a.y - 0.5 * t1.y);
+  const double2 r = make_double2(s * t2.y, -s * t2.x);  // -i s (b - c)
+  a = cadd(a, t1);
+  b = cadd(m, r);
+  c = csub(m, r);
+}
+
+__device__ __forceinline__ void dft4(double2& a0, double2& a1, double2& a2, double2& a3) {
+  const double2 s0 = cadd(a0, a2), d0 = csub(a0, a2);
+  const double2 s1 = cadd(a1, a3), d1 = cmul_mi(csub(a1, a3));
+  a0 = cadd(s0, s1);
+  a2 = csub(s0, s1);
+  a1 = cadd(d0, d1);
+  a3 = csub(d0, d1);
+}
+
+__device__ __forceinline__ void dft8(double2* v) {
+  const double c = 0.70710678118654752440;  // sqrt(1/2)
+  double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4(e0, e1, e2, e3);
+  dft4(o0, o1, o2, o3);
+  o1 = make_double2(c * (o1.x + o1.y), c * (o1.y - o1.x));   // e^{-i pi/4} o1
+  o2 = cmul_mi(o2);                                          // e^{-i pi/2} o2
+  o3 = make_double2(c * (o3.y - o3.x), -c * (o3.x + o3.y));  // e^{-3i pi/4} o3
+  v[0] = cadd(e0, o0);
+  v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1);
+  v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2);
+  v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3);
+  v[7] = csub(e3, o3);
+}
+
+// Padded position of complex element m of a line in shared memory: one empty
+// slot after every 8 elements, so the strided stores of the first stages hit
+// distinct banks.
+__device__ __forceinline__ int pz(int m) { return m + (m >> 3); }
+
+// Shared-memory geometry for complex line length P: two buffers of
+// dst_bufd(P) doubles; line t of a complex buffer starts at t dst_lp(P); the
+// result tile keeps output 2k (even region, from 0) and 2k+1 (odd region,
+// from dst_odd(P)) of line t at k (kDstLines + 1) + t. The odd region starts
+// 8 doubles past a multiple of 16, so the even and odd halves of a warp's
+// reads fall in different banks.
+__host__ __device__ constexpr int dst_lp(int P) { return P + ((P + 7) >> 3); }
+__host__ __device__ constexpr int dst_odd(int P) { return ((P * (kDstLines + 1) + 15) & ~15) + 8; }
+__host__ __device__ constexpr int dst_bufd(int P) {
+  return ((2 * kDstLines * dst_lp(P) > dst_odd(P) + (P - 1) * (kDstLines + 1)
+               ? 2 * kDstLines * dst_lp(P)
+               : dst_odd(P) + (P - 1) * (kDstLines + 1)) +
+          1) &
+         ~1;
+}
+// Radix of the next stage for a remaining length q: all 8s, then 4, 2, 3,
+// then other primes (the order the plan's factorisation uses).
+__host__ __device__ constexpr int dst_radix(int q) {
+  return q % 8 == 0 ? 8 : q % 4 == 0 ? 4 : q % 2 == 0 ? 2 : q % 3 == 0 ? 3 : q;
+}
+
+// One Stockham stage of radix R over the CTA's lines: sub-transforms of length
+// Ns (done) combine into length Ns*R. Butterfly j reads s[j + r P/R], applies
+// the twiddle e^{-2 pi i r (j mod Ns)/(Ns R)} (tw[k] = e^{-2 pi i k/N}, tstep =
+// N/(Ns R)) and writes d[(j div Ns) Ns R + (j mod Ns) + r Ns]. LP is the
+// padded line stride. Inlined with constant sizes, the index arithmetic folds.
+template <int R>
+__device__ __forceinline__ void stockham_stage(const double2* __restrict__ s, double2* __restrict__ d,
+                                               int P, int LP, int Ns, int tstep,
+                                               const double2* __restrict__ tw) {
+  const int Q = P / R;
+  for (int task = threadIdx.x; task < kDstLines * Q; task += kDstThreads) {
+    const int t = task / Q, j = task - t * Q;
+    const int jm = j % Ns;
+    const double2* sl = s + t * LP;
+    double2* dl = d + t * LP;
+    const int base = (j - jm) * R + jm;
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = sl[pz(j + r * Q)];
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) v[r] = cmul(v[r], __ldg(&tw[r * jm * tstep]));
     }
-    y[idx] = v;
+    if constexpr (R == 2) dft2(v[0], v[1]);
+    else if constexpr (R == 3) dft3(v[0], v[1], v[2]);
+    else if constexpr (R == 4) dft4(v[0], v[1], v[2], v[3]);
+    else dft8(v);
+#pragma unroll
+    for (int r = 0; r < R; r++) dl[pz(base + r * Ns)] = v[r];
   }
 }
 
-// mode 0: plain; mode 1: divide by eigenvalue (i,j,k) = (k_line, line -> (j,k));
-// mode 2: scale and add into u grid (N+1)^3 at interior offset, u pre-filled with w.
-__global__ void dst_post_kernel(long lines, int n, const double2* __restrict__ Z,
-                                double* __restrict__ out, int mode, const double* __restrict__ evc,
-                                const double* __restrict__ evs, double scale,
-                                const double* __restrict__ w, double* __restrict__ u) {
-  const int N = n + 1;
-  const int H = N / 2;
-  long l = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (l >= lines) return;
-  const double2* z = Z + l * (H + 1);
-  // line l of the input [a][b][c] layout is (a, b) = (l / nb, l % nb) with
-  // nb = n; the output position of element k is out[k][l].
-  const long L = lines;
-  int ja = 0, jb = 0;
-  double sa = 0, ca = 0, sb = 0, cb = 0;
-  if (mode != 0) {
-    ja = (int)(l / n);
-    jb = (int)(l % n);
-    ca = evc[ja];
-    sa = evs[ja];
-    cb = evc[jb];
-    sb = evs[jb];
-  }
-  auto emit = [&](int k, double F2) {
-    // F2 = 2 F_{k+1}: RODFT00 output index k
-    if (mode == 0) {
-      out[(long)k * L + l] = F2;
-    } else if (mode == 1) {
-      // factor for (i, j, k) = (k, ja, jb) (E2G/main.cpp:1447-1476)
-      double c1 = evc[k], s1 = evs[k];
-      double lap7 = s1 + sa + sb;
-      double sum8 = c1 * ca * cb;
-      double factor = 2.0 / 3.0 * (2.0 * lap7 + sum8 - 1.0);
-      double v = F2;
-      if (fabs(factor) > 1.e-14) v /= factor;
-      else v = 0.0;
-      out[(long)k * L + l] = v;
-    } else {
-      const int M = n + 2;  // grid size N_grid + 1
-      long gi = ((long)(k + 1) * M + (ja + 1)) * M + (jb + 1);
-      u[gi] = w[gi] + F2 * scale;
+// The same stage for any other (prime) radix, as a direct R-point DFT read
+// straight from shared memory.
+__device__ void stockham_stage_any(const double2* __restrict__ s, double2* __restrict__ d, int P, int LP,
+                                   int R, int Ns, int tstep, int N, const double2* __restrict__ tw) {
+  const int Q = P / R, NR = N / R;
+  for (int task = threadIdx.x; task < kDstLines * Q; task += kDstThreads) {
+    const int t = task / Q, j = task - t * Q;
+    const int jm = j % Ns;
+    const double2* sl = s + t * LP;
+    double2* dl = d + t * LP;
+    const int base = (j - jm) * R + jm;
+    for (int rp = 0; rp < R; rp++) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int r = 0; r < R; r++) {
+        int e = r * jm * tstep + ((r * rp) % R) * NR;  // both terms < N
+        if (e >= N) e -= N;
+        acc = cadd(acc, cmul(sl[pz(j + r * Q)], __ldg(&tw[e])));
+      }
+      dl[pz(base + rp * Ns)] = acc;
     }
-  };
-  double2 z0 = z[0];
-  double Fodd = z0.x;  // 2 F_1 = R_0
-  emit(0, Fodd);
-  for (int k = 1; k < H; k++) {
-    double2 zk = z[k];
-    emit(2 * k - 1, -2.0 * zk.y);  // 2 F_{2k} = -2 I_k
-    Fodd += 2.0 * zk.x;            // 2 F_{2k+1} = 2 F_{2k-1} + 2 R_k
-    if (2 * k < n) emit(2 * k, Fodd);
+  }
+}
+
+// All stages of a compile-time line length P (radices 8, 4, 2, 3 only).
+template <int P, int Ns>
+__device__ __forceinline__ void fft_fixed(double2*& s, double2*& d, const double2* __restrict__ tw) {
+  if constexpr (Ns < P) {
+    constexpr int R = dst_radix(P / Ns);
+    static_assert(R == 2 || R == 3 || R == 4 || R == 8, "compile-time line lengths factor into 2, 3");
+    stockham_stage<R>(s, d, P, dst_lp(P), Ns, 2 * P / (Ns * R), tw);
+    __syncthreads();
+    double2* x = s;
+    s = d;
+    d = x;
+    fft_fixed<P, Ns * R>(s, d, tw);
+  }
+}
+
+// One DST-I pass over n^2 lines of n points (n + 1 even), written rotated.
+// PF > 0 compiles the pass for complex length P = PF (n = 2 PF - 1), PF = 0
+// takes any n with the radices in `rad`.
+// mode 0: out[k][l] = 2F_k; 1: divided by the eigenvalue of grid point
+// (k, l div n, l mod n) (E2G/main.cpp:1445-1476); 2: u = w + scale 2F_k at the
+// interior point (k+1, l div n + 1, l mod n + 1) of the (n+2)^3 grid; 3:
+// out[k][l] = scale 2F_k.
+template <int PF>
+__global__ void __launch_bounds__(kDstThreads, 4)
+    dst_pass_kernel(int n_rt, DstRadix rad, const double* __restrict__ in, double* __restrict__ out, int mode,
+                    const double2* __restrict__ tw, const double* __restrict__ sintab,
+                    const double* __restrict__ evc, const double* __restrict__ evs, double scale,
+                    const double* __restrict__ w, double* __restrict__ u) {
+  extern __shared__ __align__(16) double dsm[];
+  constexpr int T = kDstLines;
+  constexpr int RS = T + 1;
+  const int n = PF > 0 ? 2 * PF - 1 : n_rt;
+  const int N = n + 1, P = N / 2;
+  const int LP = dst_lp(P);
+  const long lines = (long)n * n;
+  const long l0 = (long)blockIdx.x * T;
+  const int nt = (int)min((long)T, lines - l0);
+
+  // 1. the auxiliary sequence: y_j is component j mod 2 of complex j div 2
+  {
+    const double* src = in + l0 * n;
+    for (int idx = threadIdx.x; idx < T * N; idx += kDstThreads) {
+      const int t = idx / N, j = idx - t * N;
+      double v = 0.0;
+      if (t < nt && j > 0) {
+        const double* row = src + t * n;
+        const double xj = row[j - 1], xm = row[N - j - 1];
+        v = __ldg(&sintab[j]) * (xj + xm) + 0.5 * (xj - xm);
+      }
+      dsm[2 * (t * LP + pz(j >> 1)) + (j & 1)] = v;
+    }
+  }
+  __syncthreads();
+
+  // 2. length-P complex FFT of each line
+  double2* s = reinterpret_cast<double2*>(dsm);
+  double2* d = reinterpret_cast<double2*>(dsm + dst_bufd(P));
+  if constexpr (PF > 0) {
+    fft_fixed<PF, 1>(s, d, tw);
+  } else {
+    int Ns = 1;
+    for (int st = 0; st < rad.nst; st++) {
+      const int R = rad.r[st];
+      const int tstep = N / (Ns * R);
+      switch (R) {
+        case 8: stockham_stage<8>(s, d, P, LP, Ns, tstep, tw); break;
+        case 4: stockham_stage<4>(s, d, P, LP, Ns, tstep, tw); break;
+        case 2: stockham_stage<2>(s, d, P, LP, Ns, tstep, tw); break;
+        case 3: stockham_stage<3>(s, d, P, LP, Ns, tstep, tw); break;
+        default: stockham_stage_any(s, d, P, LP, R, Ns, tstep, N, tw); break;
+      }
+      __syncthreads();
+      double2* x = s;
+      s = d;
+      d = x;
+      Ns *= R;
+    }
+  }
+
+  // 3. real split and the odd-index recurrence (a warp per line, 32
+  // consecutive k per round, carried prefix sum across rounds)
+  double* ev = reinterpret_cast<double*>(d);
+  double* od = ev + dst_odd(P);
+  {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int t = warp; t < T; t += kDstThreads / 32) {
+      const double2* Z = s + t * LP;
+      const double2 z0 = Z[0];
+      const double R0 = z0.x + z0.y;
+      if (lane == 0) ev[t] = R0;
+      double carry = R0;
+      for (int kb = 1; kb < P; kb += 32) {
+        const int k = kb + lane;
+        double v = 0.0;
+        if (k < P) {
+          const double2 a = Z[pz(k)], b = Z[pz(P - k)];
+          const double Ex = 0.5 * (a.x + b.x), Ey = 0.5 * (a.y - b.y);
+          const double Ox = 0.5 * (a.y + b.y), Oy = -0.5 * (a.x - b.x);
+          const double2 wk = __ldg(&tw[k]);
+          const double Yx = Ex + (wk.x * Ox - wk.y * Oy);
+          const double Yy = Ey + (wk.x * Oy + wk.y * Ox);
+          od[(k - 1) * RS + t] = -2.0 * Yy;
+          v = 2.0 * Yx;
+        }
+        double incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const double x = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += x;
+        }
+        if (k < P) ev[k * RS + t] = carry + incl;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+      }
+    }
+  }
+  __syncthreads();
+
+  // 4. rotated stores with the pass's epilogue; output kk = 2k + parity
+  for (int idx = threadIdx.x; idx < n * T; idx += kDstThreads) {
+    const int kk = idx / T, t = idx - kk * T;
+    if (t >= nt) continue;
+    const long l = l0 + t;
+    const double F2 = ((kk & 1) ? od : ev)[(kk >> 1) * RS + t];
+    if (mode == 0) {
+      out[kk * lines + l] = F2;
+    } else if (mode == 3) {
+      out[kk * lines + l] = F2 * scale;
+    } else {
+      const int ja = (int)l / n, jb = (int)l - ja * n;
+      if (mode == 1) {
+        const double c1 = __ldg(&evc[kk]), s1 = __ldg(&evs[kk]);
+        const double ca = __ldg(&evc[ja]), sa = __ldg(&evs[ja]);
+        const double cb = __ldg(&evc[jb]), sb = __ldg(&evs[jb]);
+        const double lap7 = s1 + sa + sb;
+        const double sum8 = c1 * ca * cb;
+        const double factor = 2.0 / 3.0 * (2.0 * lap7 + sum8 - 1.0);
+        double v = F2;
+        if (fabs(factor) > 1.e-14) v /= factor;
+        else v = 0.0;
+        out[kk * lines + l] = v;
+      } else {
+        const long M = n + 2;  // grid size N_grid + 1
+        const long gi = ((long)(kk + 1) * M + (ja + 1)) * M + (jb + 1);
+        u[gi] = w[gi] + F2 * scale;
+      }
+    }
   }
 }
 
 // Transfinite (Coons) extension of the boundary values (extend_into_cube,
-// E2G/main.cpp:1494-1527).
-__global__ void extend_kernel(int N, double L, double h, const double* __restrict__ g,
-                              double* __restrict__ G) {
+// E2G/main.cpp:1494-1527):
+//   G = F - E1 - E2 - E3 + C,  F = x g(N,j,k) + (1-x) g(0,j,k) + y g(i,N,k)
+//   + (1-y) g(i,0,k) + z g(i,j,N) + (1-z) g(i,j,0), E1..E3 the bilinear edge
+//   terms, C the trilinear corner term, x, y, z = i h/L, j h/L, k h/L.
+// Along a grid row (i, j) every term that does not read a k-dependent boundary
+// value is linear in z, so a row is
+//   G(k) = x g(N,j,k) + (1-x) g(0,j,k) + y g(i,N,k) + (1-y) g(i,0,k)
+//          - E3(k) + K0 + z K1,
+// with K0, K1 formed once per row. One CTA per (j, kExtRows rows of i).
+constexpr int kExtRows = 16;
+
+__global__ void __launch_bounds__(128) extend_kernel(int N, double L, double h, const double* __restrict__ g,
+                                                     double* __restrict__ G) {
+  __shared__ double row[kExtRows][7];  // x, E3 weights (4), K0, K1
   const long M = N + 1;
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= M * M * M) return;
-  int i = (int)(idx / (M * M)), j = (int)((idx / M) % M), k = (int)(idx % M);
+  const int j = blockIdx.x;
+  const int ia = blockIdx.y * kExtRows, nr = min(N + 1 - ia, kExtRows);
   auto at = [&](int a, int b, int c) { return g[((long)a * M + b) * M + c]; };
-  double x = i * h / L, y = j * h / L, z = k * h / L;
-  double F, E1, E2, E3, C;
-  F = x * at(N, j, k) + (1.0 - x) * at(0, j, k);
-  F += y * at(i, N, k) + (1.0 - y) * at(i, 0, k);
-  F += z * at(i, j, N) + (1.0 - z) * at(i, j, 0);
-  E1 = (1.0 - y) * (1.0 - z) * at(i, 0, 0) + (1.0 - y) * z * at(i, 0, N) +
-       y * (1.0 - z) * at(i, N, 0) + y * z * at(i, N, N);
-  E2 = (1.0 - x) * (1.0 - z) * at(0, j, 0) + (1.0 - x) * z * at(0, j, N) +
-       x * (1.0 - z) * at(N, j, 0) + x * z * at(N, j, N);
-  E3 = (1.0 - x) * (1.0 - y) * at(0, 0, k) + (1.0 - x) * y * at(0, N, k) +
-       x * (1.0 - y) * at(N, 0, k) + x * y * at(N, N, k);
-  C = (1.0 - x) * (1.0 - y) * (1.0 - z) * at(0, 0, 0) + (1.0 - x) * (1.0 - y) * z * at(0, 0, N) +
-      (1.0 - x) * y * (1.0 - z) * at(0, N, 0) + (1.0 - x) * y * z * at(0, N, N) +
-      x * (1.0 - y) * (1.0 - z) * at(N, 0, 0) + x * (1.0 - y) * z * at(N, 0, N) +
-      x * y * (1.0 - z) * at(N, N, 0) + x * y * z * at(N, N, N);
-  G[idx] = F - E1 - E2 - E3 + C;
+  const double y = j * h / L;
+  if (threadIdx.x < nr) {
+    const int i = ia + threadIdx.x;
+    const double x = i * h / L;
+    const double b0 = at(i, j, 0), bN = at(i, j, N);
+    const double c1 = at(i, 0, 0), c2 = at(i, 0, N), c3 = at(i, N, 0), c4 = at(i, N, N);
+    const double d1 = at(0, j, 0), d2 = at(0, j, N), d3 = at(N, j, 0), d4 = at(N, j, N);
+    const double w00 = (1.0 - x) * (1.0 - y), w0N = (1.0 - x) * y, wN0 = x * (1.0 - y), wNN = x * y;
+    const double Ca = w00 * at(0, 0, 0) + w0N * at(0, N, 0) + wN0 * at(N, 0, 0) + wNN * at(N, N, 0);
+    const double Cb = w00 * (at(0, 0, N) - at(0, 0, 0)) + w0N * (at(0, N, N) - at(0, N, 0)) +
+                      wN0 * (at(N, 0, N) - at(N, 0, 0)) + wNN * (at(N, N, N) - at(N, N, 0));
+    const double E1a = (1.0 - y) * c1 + y * c3, E1b = (1.0 - y) * (c2 - c1) + y * (c4 - c3);
+    const double E2a = (1.0 - x) * d1 + x * d3, E2b = (1.0 - x) * (d2 - d1) + x * (d4 - d3);
+    double* r = row[threadIdx.x];
+    r[0] = x;
+    r[1] = w00;
+    r[2] = w0N;
+    r[3] = wN0;
+    r[4] = wNN;
+    r[5] = b0 - E1a - E2a + Ca;
+    r[6] = (bN - b0) - E1b - E2b + Cb;
+  }
+  __syncthreads();
+  const double* fN = g + ((long)N * M + j) * M;  // g(N, j, .)
+  const double* f0 = g + (long)j * M;            // g(0, j, .)
+  const double* e00 = g;                         // g(0, 0, .)
+  const double* e0N = g + (long)N * M;           // g(0, N, .)
+  const double* eN0 = g + (long)N * M * M;       // g(N, 0, .)
+  const double* eNN = eN0 + (long)N * M;         // g(N, N, .)
+  for (int k = threadIdx.x; k <= N; k += blockDim.x) {
+    const double z = k * h / L;
+    const double vN = fN[k], v0 = f0[k];
+    const double q00 = e00[k], q0N = e0N[k], qN0 = eN0[k], qNN = eNN[k];
+    for (int r = 0; r < nr; r++) {
+      const int i = ia + r;
+      const double* gi = g + (long)i * M * M;
+      const double* R = row[r];
+      const double x = R[0];
+      const double E3 = R[1] * q00 + R[2] * q0N + R[3] * qN0 + R[4] * qNN;
+      const double F = x * vN + (1.0 - x) * v0 + y * gi[(long)N * M + k] + (1.0 - y) * gi[k];
+      G[((long)i * M + j) * M + k] = F - E3 + (R[5] + z * R[6]);
+    }
+  }
 }
 
 // 4th-order compact Laplacian RHS (lapl_4ord_inCube, lapl_4ord_nearSurfc,
 // dp_d{x,y,z}_4ord: E2G/main.cpp:1566-1823), one fused pass over the interior.
-__global__ void rhs_kernel(int N, double h, const double* __restrict__ Gw,
-                           const double* __restrict__ u, const uint8_t* __restrict__ band2,
-                           const uint8_t* __restrict__ outside, const double* __restrict__ p,
-                           int axis, double* __restrict__ rhs) {
+// One CTA per interior row (i, j), threads along k, each of the nine
+// neighbouring rows of w and u addressed from its own row pointer.
+__global__ void __launch_bounds__(128)
+    rhs_kernel(int N, double h, const double* __restrict__ Gw, const double* __restrict__ u,
+               const uint8_t* __restrict__ band2, const uint8_t* __restrict__ outside,
+               const double* __restrict__ p, int axis, double* __restrict__ rhs) {
   const long M = N + 1;
   const long n = N - 1;
-  long idx = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= n * n * n) return;
-  int i = (int)(idx / (n * n)) + 1, j = (int)((idx / n) % n) + 1, k = (int)(idx % n) + 1;
-  auto G = [&](const double* a, int ii, int jj, int kk) { return a[((long)ii * M + jj) * M + kk]; };
-  auto lap = [&](const double* a) {
-    double lap7 = G(a, i + 1, j, k) + G(a, i - 1, j, k) + G(a, i, j + 1, k) + G(a, i, j - 1, k) +
-                  G(a, i, j, k + 1) + G(a, i, j, k - 1) - 6.0 * G(a, i, j, k);
-    double temp1 = G(a, i + 1, j + 1, k + 1) + G(a, i + 1, j - 1, k + 1) +
-                   G(a, i - 1, j + 1, k + 1) + G(a, i - 1, j - 1, k + 1) - 4.0 * G(a, i, j, k);
-    double temp2 = G(a, i + 1, j + 1, k - 1) + G(a, i + 1, j - 1, k - 1) +
-                   G(a, i - 1, j + 1, k - 1) + G(a, i - 1, j - 1, k - 1) - 4.0 * G(a, i, j, k);
+  const int j = blockIdx.x + 1, i = blockIdx.y + 1;
+  const long c0 = ((long)i * M + j) * M;  // row (i, j)
+  const long sj = M, si = M * M;
+  const long gst = axis == 0 ? si : (axis == 1 ? sj : 1);
+  const int c = axis == 0 ? i : (axis == 1 ? j : 0);
+  double* out = rhs + ((long)(i - 1) * n + (j - 1)) * n;  // out[k - 1] = rhs(i, j, k)
+  auto lap = [&](const double* a, int k) {
+    const double* r0 = a + c0 + k;
+    const double ctr = r0[0];
+    double lap7 = r0[si] + r0[-si] + r0[sj] + r0[-sj] + r0[1] + r0[-1] - 6.0 * ctr;
+    double temp1 = r0[si + sj + 1] + r0[si - sj + 1] + r0[-si + sj + 1] + r0[-si - sj + 1] - 4.0 * ctr;
+    double temp2 = r0[si + sj - 1] + r0[si - sj - 1] + r0[-si + sj - 1] + r0[-si - sj - 1] - 4.0 * ctr;
     return lap7 + (temp1 + temp2) / 8.0;
   };
-  double r = -2.0 / 3.0 * lap(Gw);
-  const long gi = ((long)i * M + j) * M + k;
-  if (band2[gi]) r += 2.0 / 3.0 * lap(u);
-  if (axis >= 0 && outside[gi]) {
-    const int c = axis == 0 ? i : (axis == 1 ? j : k);
-    const int di = axis == 0, dj = axis == 1, dk = axis == 2;
-    auto P = [&](int o) { return G(p, i + o * di, j + o * dj, k + o * dk); };
-    double d;
-    if (c == 0 || c == 1) {
-      d = -(25.0 / 12.0) * P(0) + 4.0 * P(1) - 3.0 * P(2) + (4.0 / 3.0) * P(3) - 0.25 * P(4);
-    } else if (c == N || c == (N - 1)) {
-      d = (25.0 / 12.0) * P(0) - 4.0 * P(-1) + 3.0 * P(-2) - (4.0 / 3.0) * P(-3) + 0.25 * P(-4);
-    } else {
-      d = -P(2) + 8.0 * P(1) - 8.0 * P(-1) + P(-2);
-      d /= 12.0;
+  for (int k = threadIdx.x + 1; k < N; k += blockDim.x) {
+    double r = -2.0 / 3.0 * lap(Gw, k);
+    if (band2[c0 + k]) r += 2.0 / 3.0 * lap(u, k);
+    if (axis >= 0 && outside[c0 + k]) {
+      const int cc = axis == 2 ? k : c;
+      const double* pc = p + c0 + k;
+      auto P = [&](int o) { return pc[o * gst]; };
+      double d;
+      if (cc == 0 || cc == 1) {
+        d = -(25.0 / 12.0) * P(0) + 4.0 * P(1) - 3.0 * P(2) + (4.0 / 3.0) * P(3) - 0.25 * P(4);
+      } else if (cc == N || cc == (N - 1)) {
+        d = (25.0 / 12.0) * P(0) - 4.0 * P(-1) + 3.0 * P(-2) - (4.0 / 3.0) * P(-3) + 0.25 * P(-4);
+      } else {
+        d = -P(2) + 8.0 * P(1) - 8.0 * P(-1) + P(-2);
+        d /= 12.0;
+      }
+      r += d * h;
     }
-    r += d * h;
+    out[k - 1] = r;
   }
-  rhs[idx] = r;
 }
+
+// u = w on the six boundary faces of the M^3 grid (the interior gets
+// w + solution from the last DST pass).
+__global__ void faces_copy_kernel(int M, const double* __restrict__ w, double* __restrict__ u) {
+  const int a = blockIdx.x, f = blockIdx.y;
+  const int c = (f & 1) ? M - 1 : 0;
+  for (int b = threadIdx.x; b < M; b += blockDim.x) {
+    long gi;
+    if ((f >> 1) == 0) gi = ((long)c * M + a) * M + b;
+    else if ((f >> 1) == 1) gi = ((long)a * M + c) * M + b;
+    else gi = ((long)a * M + b) * M + c;
+    u[gi] = w[gi];
+  }
+}
+
+using PassFn = void (*)(int, DstRadix, const double*, double*, int, const double2*, const double*,
+                       const double*, const double*, double, const double*, double*);
 
 struct DstPlan {
   int n = 0;
-  cufftHandle plan = 0;
-  DBuf<double> y, sintab, evc, evs;
-  DBuf<double2> z;
-  DBuf<double> tmp;
+  size_t smem = 0;
+  DstRadix rad{};
+  PassFn fn = nullptr;
+  DBuf<double> sintab, evc, evs, tmp;
+  DBuf<double2> tw;
   void make(Ctx& C, int n_) {
     n = n_;
     const int N = n + 1;
-    HR_REQUIRE(N % 2 == 0, "DST-I via real FFT needs n + 1 even");
-    const long lines = (long)n * n;
-    int dims[1] = {N};
-    int inembed[1] = {N}, onembed[1] = {N / 2 + 1};
-    HR_CHECK_CUFFT(cufftPlanMany(&plan, 1, dims, inembed, 1, N, onembed, 1, N / 2 + 1, CUFFT_D2Z,
-                                 (int)lines));
-    HR_CHECK_CUFFT(cufftSetStream(plan, C.stream));
-    y.alloc((size_t)lines * N);
-    z.alloc((size_t)lines * (N / 2 + 1));
+    HR_REQUIRE(N % 2 == 0, "DST-I via a half-length complex FFT needs n + 1 even");
+    const int P = N / 2;
+    rad.nst = 0;
+    for (int q = P; q > 1;) {
+      int f = dst_radix(q);
+      if (q % 2 != 0 && q % 3 != 0)  // q's smallest prime factor, 5 or above
+        for (f = 5; q % f; f += 2) {}
+      HR_REQUIRE(rad.nst < kDstMaxStages, "DST-I length has too many factors");
+      rad.r[rad.nst++] = f;
+      q /= f;
+    }
+    smem = 2 * (size_t)dst_bufd(P) * sizeof(double);
+    HR_REQUIRE(smem <= 227 * 1024, "DST-I line longer than one CTA's shared memory holds");
+    // the grid sizes of the benchmark workloads (N = 48, 96, 384) run passes
+    // compiled for their line length
+    fn = P == 192 ? dst_pass_kernel<192> : P == 48 ? dst_pass_kernel<48> : P == 24 ? dst_pass_kernel<24>
+                                                                                    : dst_pass_kernel<0>;
+    HR_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     tmp.alloc((size_t)n * n * n);
+    // twiddles e^{-2 pi i k/N} and sin(j pi/N), evaluated in extended precision
+    std::vector<double2> t(N);
     std::vector<double> st(N), c(n), s(n);
-    for (int j = 0; j < N; j++) st[j] = sin(j * 3.14159265358979323846 / N);
+    const long double PIL = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < N; k++) {
+      const long double a = 2.0L * PIL * k / N;
+      t[k] = make_double2((double)cosl(a), (double)-sinl(a));
+      st[k] = (double)sinl(PIL * k / N);
+    }
     // eigenvalue factors exactly as E2G/main.cpp:1445-1460 evaluates them
     const double PI = 3.14159265358979323846;
     double pi_over_n = PI / (n + 1);
@@ -207,35 +501,30 @@ struct DstPlan {
       s1 *= -2.0 * s1;
       s[i] = s1;
     }
+    tw.upload(t, C.stream);
     sintab.upload(st, C.stream);
     evc.upload(c, C.stream);
     evs.upload(s, C.stream);
   }
-  ~DstPlan() {
-    if (plan) cufftDestroy(plan);
-  }
-  // one pass: in [n][n][n] -> out rotated
-  void pass(Ctx& C, const double* in, double* out, int mode, double scale, const double* w,
-            double* u) {
+  // one pass: in [n][n][n] -> out rotated (or into u for mode 2)
+  void pass(Ctx& C, const double* in, double* out, int mode, double scale, const double* w, double* u) {
     const long lines = (long)n * n;
-    const int N = n + 1;
-    long tot = lines * N;
-    int blocks = (int)std::min<long>((tot + 255) / 256, 148L * 32);
-    dst_pre_kernel<<<blocks, 256, 0, C.stream>>>(lines, n, in, sintab.p, y.p);
-    HR_CHECK_CUFFT(cufftExecD2Z(plan, y.p, (cufftDoubleComplex*)z.p));
-    dst_post_kernel<<<(int)((lines + 127) / 128), 128, 0, C.stream>>>(lines, n, z.p, out, mode,
-                                                                      evc.p, evs.p, scale, w, u);
-    C.launches += 3;
+    const long blocks = (lines + kDstLines - 1) / kDstLines;
+    fn<<<(unsigned)blocks, kDstThreads, smem, C.stream>>>(n, rad, in, out, mode, tw.p, sintab.p, evc.p, evs.p,
+                                                          scale, w, u);
+    C.launches++;
     HR_CHECK_CUDA(cudaGetLastError());
   }
-  // 3D DST-I of a (in place through tmp); last pass uses mode/scale/w/u
-  void dst3(Ctx& C, double* a, int last_mode, double scale, const double* w, double* u) {
-    pass(C, a, tmp.p, 0, 0, nullptr, nullptr);
-    pass(C, tmp.p, a, 0, 0, nullptr, nullptr);
-    pass(C, a, tmp.p, last_mode, scale, w, u);
-    if (last_mode != 2)
-      HR_CHECK_CUDA(cudaMemcpyAsync(a, tmp.p, sizeof(double) * (size_t)n * n * n,
-                                    cudaMemcpyDeviceToDevice, C.stream));
+  // Forward 3D DST-I with the eigenvalue divide, then the inverse 3D DST-I:
+  // six passes alternating between a and tmp, starting and ending at a; the
+  // last pass writes with `last_mode` (2: into u, 3: scaled into a).
+  void solve(Ctx& C, double* a, int last_mode, double scale, const double* w, double* u) {
+    pass(C, a, tmp.p, 0, 0.0, nullptr, nullptr);
+    pass(C, tmp.p, a, 0, 0.0, nullptr, nullptr);
+    pass(C, a, tmp.p, 1, 0.0, nullptr, nullptr);
+    pass(C, tmp.p, a, 0, 0.0, nullptr, nullptr);
+    pass(C, a, tmp.p, 0, 0.0, nullptr, nullptr);
+    pass(C, tmp.p, a, last_mode, scale, w, u);
   }
 };
 
@@ -244,16 +533,13 @@ struct DstPlan {
 void dst_poisson3d_dev(Ctx& C, int n, double* f_dev) {
   DstPlan P;
   P.make(C, n);
-  P.dst3(C, f_dev, 1, 0.0, nullptr, nullptr);
-  P.dst3(C, f_dev, 0, 0.0, nullptr, nullptr);
-  double scale = 1. / pow(2 * (n + 1), 3);
-  launch_scale_host(n * n * n, scale, f_dev, C.stream);
-  C.launches++;
-  HR_CHECK_CUDA(cudaGetLastError());
+  P.solve(C, f_dev, 3, 1. / pow(2 * (n + 1), 3), nullptr, nullptr);
+  // the plan's buffers are freed at return and must be idle first
+  HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
 }
 
-// The FFT plan, twiddle tables and grid work buffers of one grid size, kept
-// across solves (a pipeline runs four solves per evaluation).
+// The twiddle tables and grid work buffers of one grid size, kept across
+// solves (a pipeline runs four solves per evaluation).
 struct PoissonWork {
   int N = 0;
   DstPlan P;
@@ -281,24 +567,18 @@ void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const 
     work = own.get();
   }
   const double h = L / N;
-  const long M = N + 1;
-  const long m3 = M * M * M;
+  const int M = N + 1;
   const int n = N - 1;
   DBuf<double>& w = work->w;
   DBuf<double>& rhs = work->rhs;
-  extend_kernel<<<(int)((m3 + 255) / 256), 256, 0, C.stream>>>(N, L, h, u_dev, w.p);
+  extend_kernel<<<dim3(M, (M + kExtRows - 1) / kExtRows), 128, 0, C.stream>>>(N, L, h, u_dev, w.p);
   const int axis = (variable >= 1 && variable <= 3) ? variable - 1 : -1;
-  long n3 = (long)n * n * n;
-  rhs_kernel<<<(int)((n3 + 255) / 256), 256, 0, C.stream>>>(N, h, w.p, u_dev, band2_dev, out_dev,
-                                                            p_dev, axis, rhs.p);
-  C.launches += 2;
+  rhs_kernel<<<dim3(n, n), 128, 0, C.stream>>>(N, h, w.p, u_dev, band2_dev, out_dev, p_dev, axis, rhs.p);
+  // u = w on the boundary; the interior gets w + the scaled solution
+  faces_copy_kernel<<<dim3(M, 6), 128, 0, C.stream>>>(M, w.p, u_dev);
+  C.launches += 3;
   HR_CHECK_CUDA(cudaGetLastError());
-  DstPlan& P = work->P;
-  P.dst3(C, rhs.p, 1, 0.0, nullptr, nullptr);
-  // u = w everywhere, then the interior gets w + scaled solution
-  HR_CHECK_CUDA(cudaMemcpyAsync(u_dev, w.p, sizeof(double) * m3, cudaMemcpyDeviceToDevice, C.stream));
-  double scale = 1. / pow(2 * (n + 1), 3);
-  P.dst3(C, rhs.p, 2, scale, w.p, u_dev);
+  work->P.solve(C, rhs.p, 2, 1. / pow(2 * (n + 1), 3), w.p, u_dev);
   // a temporary work area is freed at return; its buffers must be idle first
   if (own) HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
 }

@@ -1,6 +1,7 @@
-"""GPU parity of the extend-to-grid Poisson path (DST-I via cuFFT with
-pre/post-twiddle kernels, 4th-order compact RHS) against the reference's
-golden outputs (E2G/main.cpp:969-1044, 1423-1823)."""
+"""GPU parity of the extend-to-grid Poisson path (fused DST-I pass kernel:
+sine pre-twiddle, shared-memory Stockham FFT, real split and recurrence;
+4th-order compact RHS) against the reference's golden outputs
+(E2G/main.cpp:969-1044, 1423-1823)."""
 import numpy as np
 import pytest
 
@@ -21,6 +22,37 @@ def test_dst_poisson_round_trip(ctx, oracle):
     n = 23
     f = np.random.default_rng(5).standard_normal(n ** 3)
     assert rel_err(ctx.dst_poisson3d(n, f), oracle.dst_poisson(n, f)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [1, 3, 5, 13, 21, 47, 95, 127, 193])
+def test_dst_poisson_line_lengths(ctx, oracle, n):
+    # every FFT stage kind: none (n = 1), radix 2, 3, 4, 8 and direct prime
+    # stages (7, 11, 97), against the oracle's direct O(n^4) transform
+    f = np.random.default_rng(n).standard_normal(n ** 3)
+    assert rel_err(ctx.dst_poisson3d(n, f), oracle.dst_poisson(n, f)) < 1e-12
+
+
+def test_dst_poisson_full_size_operator(ctx):
+    # n = 383, the line length of the N = 384 grid: the 4th-order compact
+    # operator (2/3)(lap7 + (sum of the 8 corners - 8u)/8) applied to the
+    # zero-padded solution returns the data
+    n = 383
+    f = np.random.default_rng(383).standard_normal(n ** 3)
+    U = np.zeros((n + 2,) * 3)
+    U[1:-1, 1:-1, 1:-1] = ctx.dst_poisson3d(n, f).reshape(n, n, n)
+    c = U[1:-1, 1:-1, 1:-1]
+    S = slice(1, -1)
+    sh = {-1: slice(0, -2), 0: S, 1: slice(2, None)}
+    Lu = -6.0 * c
+    for a, b, e in ((1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+        Lu += U[sh[a], sh[b], sh[e]]
+    Lu -= c
+    for a in (-1, 1):
+        for b in (-1, 1):
+            for e in (-1, 1):
+                Lu += U[sh[a], sh[b], sh[e]] / 8.0
+    Lu *= 2.0 / 3.0
+    assert rel_err(Lu.ravel(), f) < 1e-9
 
 
 def test_solve_poisson_matches_reference(ctx, ge2g):
