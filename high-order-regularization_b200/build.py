@@ -2,8 +2,8 @@
 
 CUDA sources are compiled with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -O3 -lineinfo``; the host
-planner (host/*.cpp) with g++ and OpenMP; the library links cuFFT and the CUDA
-runtime. Objects go to ``_build/`` next to this file; the shared library sits
+planner (host/*.cpp) with g++ and OpenMP; the library links the CUDA runtime
+(static) and OpenMP. Objects go to ``_build/`` next to this file; the shared library sits
 next to this file so that it travels with the working tree.
 """
 from __future__ import annotations

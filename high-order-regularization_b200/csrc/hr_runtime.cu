@@ -1,11 +1,73 @@
 // hr_runtime.cu — device trees, target lists, stencils and evaluation batches.
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <numeric>
 
 #include "hr_runtime.h"
 
 namespace hr {
+
+namespace {
+
+// Freed blocks the pool keeps mapped before it returns memory to the driver.
+constexpr uint64_t kPoolKeepBytes = 8ull << 30;
+constexpr int kMaxDevices = 64;
+
+struct DevPool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t st = nullptr;  // the pool's own stream: allocations and frees only
+};
+
+std::mutex g_pool_mu;
+DevPool g_pools[kMaxDevices];
+
+DevPool& pool_of(int dev) {
+  HR_REQUIRE(dev >= 0 && dev < kMaxDevices, "device index out of range");
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  DevPool& P = g_pools[dev];
+  if (!P.pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    HR_CHECK_CUDA(cudaMemPoolCreate(&P.pool, &props));
+    uint64_t keep = kPoolKeepBytes;
+    HR_CHECK_CUDA(cudaMemPoolSetAttribute(P.pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    HR_CHECK_CUDA(cudaStreamCreateWithFlags(&P.st, cudaStreamNonBlocking));
+  }
+  return P;
+}
+
+}  // namespace
+
+void* dev_alloc(size_t bytes) {
+  int dev = 0;
+  HR_CHECK_CUDA(cudaGetDevice(&dev));
+  DevPool& P = pool_of(dev);
+  void* p = nullptr;
+  HR_CHECK_CUDA(cudaMallocFromPoolAsync(&p, bytes, P.pool, P.st));
+  // complete before any other stream sees the pointer
+  HR_CHECK_CUDA(cudaStreamSynchronize(P.st));
+  return p;
+}
+
+void dev_free(void* p) noexcept {
+  if (!p) return;
+  try {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess || a.type != cudaMemoryTypeDevice) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (a.device != cur) cudaSetDevice(a.device);
+    cudaDeviceSynchronize();
+    DevPool& P = pool_of(a.device);
+    cudaFreeAsync(p, P.st);
+    if (a.device != cur) cudaSetDevice(cur);
+  } catch (...) {
+  }
+}
 
 void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direct,
                     cudaStream_t st) {

@@ -31,6 +31,14 @@ struct Error : std::runtime_error {
     if (!(cond)) throw ::hr::Error(HR_ERR_ARG, std::string(msg)); \
   } while (0)
 
+// The library's device buffers come from one stream-ordered memory pool per
+// device that keeps freed blocks mapped (up to a few GiB), so building and
+// destroying plans does not map and unmap pages for every buffer. dev_alloc
+// returns memory that every stream may use at once; dev_free first waits for
+// the pointer's device to go idle, as cudaFree does, and never throws.
+void* dev_alloc(size_t bytes);
+void dev_free(void* p) noexcept;
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -54,14 +62,14 @@ struct DBuf {
   }
   ~DBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p);
     p = nullptr;
     n = 0;
   }
   void alloc(size_t count) {
     release();
     if (count == 0) count = 1;
-    HR_CHECK_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    p = static_cast<T*>(dev_alloc(count * sizeof(T)));
     n = count;
   }
   void upload(const T* h, size_t count, cudaStream_t st) {
