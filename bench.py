@@ -252,7 +252,8 @@ def timed_solves(plan, stream, flush, f1, f2, b, x, prec, steps, guess=None):
         times.append(e0.elapsed_time(e1))
         reps.append(rep)
     r = reps[-1]
-    return {"ms_per_step": sum(times) / len(times), "gmres_iterations": r["iterations"],
+    return {"ms_per_step": sum(times) / len(times), "ms_min": min(times), "ms_max": max(times),
+            "gmres_iterations": r["iterations"],
             "matvecs_fp64": r["matvecs_fp64"], "matvecs_mixed": r["matvecs_mixed"], "residual": r["residual"],
             "true_residual": r["true_residual"], "guess_rejected": r["guess_rejected"]}
 
@@ -312,6 +313,8 @@ def run_ours(args, rank, world, local_rank):
     # mixed precision, and mixed precision with the learned warm start
     variants = {}
     for name, pr in (("fp64", highreg.HR_FP64), ("mixed", highreg.HR_MIXED)):
+        # one untimed solve first: the reduced-precision batches are built on first use
+        timed_solves(plan, stream, flush, f1, f2, b, x, pr, 1)
         variants[name] = timed_solves(plan, stream, flush, f1, f2, b, x, pr, args.steps)
     guess, feat_s = warm_guess_fn(ctx, geo, dev)
     if guess is not None:
