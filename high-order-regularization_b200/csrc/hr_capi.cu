@@ -455,6 +455,19 @@ struct hr_plan2s {
   std::vector<double> hxyz[2], hnrml[2], harea[2];
   std::vector<uint8_t> near_host[2];
   hr_surface surf_host[2];
+  // The FP64 stresslet batch is segmented on a host thread of its own while
+  // the caller goes on (to the right-hand side, which needs only the Stokeslet
+  // batch), its uploads on a stream of its own; every other use of the plan
+  // first waits for it (plan_ready).
+  std::thread dl_thread;
+  std::exception_ptr dl_error;
+  cudaStream_t up = nullptr;
+  cudaEvent_t up_done = nullptr;
+  ~hr_plan2s() {
+    if (dl_thread.joinable()) dl_thread.join();
+    if (up_done) cudaEventDestroy(up_done);
+    if (up) cudaStreamDestroy(up);
+  }
 };
 
 namespace {
@@ -494,8 +507,7 @@ void sl_batch(hr_plan2s& P);
 // Stresslet batches of the matvec, one per precision in [prec0, prec1), over
 // the given trees and lists (the plan's own, or the inner operator's).
 void dl_batches(hr_plan2s& P, DevTree* tree, DevLists* Lon, DevLists* Loff, Batch* dl, int prec0, int prec1,
-                bool count) {
-  cudaStream_t st = P.C->stream;
+                bool count, cudaStream_t st) {
   const bool direct = P.opt.mode == HR_DIRECT;
   for (int prec = prec0; prec < prec1; prec++) {
     Batch& B = dl[prec];
@@ -531,8 +543,31 @@ void plan_batches(hr_plan2s& P) {
   P.counters.alloc(4 * 8);
   P.counters.zero(st);
   // the reduced-precision batches are built on first use (plan_matvec); the
-  // FP64 stresslet and the Stokeslet batches are built on two host threads
-  run_both(P.C->device, [&] { dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, 1, true); }, [&] { sl_batch(P); });
+  // Stokeslet batch here, the FP64 stresslet batch on a second host thread
+  // that outlives the plan's creation
+  sl_batch(P);
+  HR_CHECK_CUDA(cudaStreamCreateWithFlags(&P.up, cudaStreamNonBlocking));
+  HR_CHECK_CUDA(cudaEventCreateWithFlags(&P.up_done, cudaEventDisableTiming));
+  const int dev = P.C->device;
+  P.dl_thread = std::thread([&P, dev] {
+    try {
+      HR_CHECK_CUDA(cudaSetDevice(dev));
+      dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, 1, true, P.up);
+      HR_CHECK_CUDA(cudaEventRecord(P.up_done, P.up));
+    } catch (...) {
+      P.dl_error = std::current_exception();
+    }
+  });
+}
+
+// Waits for the FP64 stresslet batch of plan_batches (and orders the plan's
+// stream after its uploads); rethrows its error on every use.
+void plan_ready(hr_plan2s& P) {
+  if (P.dl_thread.joinable()) {
+    P.dl_thread.join();
+    if (!P.dl_error) HR_CHECK_CUDA(cudaStreamWaitEvent(P.C->stream, P.up_done, 0));
+  }
+  if (P.dl_error) std::rethrow_exception(P.dl_error);
 }
 
 void sl_batch(hr_plan2s& P) {
@@ -572,7 +607,8 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
                   P.xin.p + P.off[1 - t], P.tg[t].g0.p, st);
     C.launches++;
   }
-  if (!in && !P.dl[prec].ready) dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, prec, prec + 1, true);
+  plan_ready(P);
+  if (!in && !P.dl[prec].ready) dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, prec, prec + 1, true, st);
   (in ? in->dl[prec] : P.dl[prec]).launch(C);
   // set 0: u - on*f - comp*f ; set 1: u - comp*f - on*f   (2S/main.cpp:612-676)
   launch_matvec_combine(3 * P.nq[0], 2.0 / 3.0, P.xin.p + P.off[0], P.out_on[0].p, P.out_off[0].p,
@@ -900,6 +936,7 @@ extern "C" int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double t
   if (!plan) return HR_ERR_ARG;
   return guard(plan->owner, [&] {
     hr_plan2s& Q = *plan;
+    plan_ready(Q);
     HR_REQUIRE(Q.opt.mode == HR_TREE, "an inner treecode needs an HR_TREE plan");
     if (rel_err) *rel_err = 0.0;
     if (P == 0) {
@@ -922,7 +959,7 @@ extern "C" int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double t
       in->Lon[t].build(in->tree[t].host, Q.nq[t], Q.surf_host[t].xyz, all.data(), st);
       in->Loff[t].build(in->tree[1 - t].host, Q.nq[t], Q.surf_host[t].xyz, Q.near_host[t].data(), st);
     }
-    dl_batches(Q, in->tree, in->Lon, in->Loff, in->dl, 1, 3, false);
+    dl_batches(Q, in->tree, in->Lon, in->Loff, in->dl, 1, 3, false, Q.C->stream);
     // accuracy of the inner operator (mixed precision) against the plan's FP64
     // one, on a fixed pseudo-random density
     Q.inner.reset();
@@ -1040,6 +1077,7 @@ extern "C" int hr_plan2s_solve(hr_plan2s* plan, const hr_gmres_opts* opt, const 
 extern "C" int hr_plan2s_work(hr_plan2s* plan, int which, hr_work* w) {
   if (!plan || !w || which < 0 || which > 2) return HR_ERR_ARG;
   return guard(ctx_of(plan), [&] {
+    plan_ready(*plan);
     if (which == 2) {
       // the inner treecode's stresslet batch, from its interaction lists (no launch)
       if (!plan->inner) throw Error(HR_ERR_STATE, "the plan has no inner treecode");
@@ -1126,6 +1164,7 @@ extern "C" int hr_measure_fp64_peak(hr_ctx* ctx, double* flops_per_s) {
 extern "C" int hr_plan2s_check_upward_pass(hr_plan2s* plan, const double* x, double* max_rel_err) {
   if (!plan || !x || !max_rel_err) return HR_ERR_ARG;
   return guard(ctx_of(plan), [&] {
+    plan_ready(*plan);
     hr_plan2s& P = *plan;
     Ctx& C = *P.C;
     cudaStream_t st = C.stream;
@@ -1194,7 +1233,9 @@ extern "C" int hr_plan2s_time_batch(hr_plan2s* plan, int which, int iters, doubl
   return guard(ctx_of(plan), [&] {
     cudaStream_t st = plan->C->stream;
     HR_REQUIRE(which != 3 || plan->inner, "the plan has no inner treecode");
-    if (which == 2 && !plan->dl[1].ready) dl_batches(*plan, plan->tree, plan->Lon, plan->Loff, plan->dl, 1, 2, true);
+    plan_ready(*plan);
+    if (which == 2 && !plan->dl[1].ready)
+      dl_batches(*plan, plan->tree, plan->Lon, plan->Loff, plan->dl, 1, 2, true, plan->C->stream);
     Batch& B = which == 3 ? plan->inner->dl[1] : which == 1 ? plan->sl : plan->dl[which == 2 ? 1 : 0];
     cudaEvent_t a, b;
     HR_CHECK_CUDA(cudaEventCreate(&a));
