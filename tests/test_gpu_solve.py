@@ -16,6 +16,21 @@ def plan16(ctx, g2s):
     p.close()
 
 
+def test_plan_lifecycle_around_the_background_batch(ctx, g2s):
+    # the FP64 stresslet batch is segmented on a host thread of its own after
+    # creation: destroying a plan at once joins it; the right-hand side runs
+    # beside it; the work counts and the first matvec wait for it
+    opt = dict(mode=highreg.HR_TREE, P=int(g2s["P"]), N0=int(g2s["N0"]), theta=0.6)
+    for _ in range(3):
+        highreg.Plan2S(ctx, g2s, **opt).close()
+    p = highreg.Plan2S(ctx, g2s, **opt)
+    b = p.rhs(g2s["f0"], g2s["f1"])
+    assert rel_err(b, g2s["rhs"]) < 1e-12
+    assert p.work(0)["direct_pairs_near"] > 0
+    assert rel_err(p.matvec(g2s["mv_u"]), g2s["mv_y"]) < 1e-12
+    p.close()
+
+
 def test_matvec_matches_reference(plan16, g2s):
     y = plan16.matvec(g2s["mv_u"])
     assert rel_err(y, g2s["mv_y"]) < 1e-12
