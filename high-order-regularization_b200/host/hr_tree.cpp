@@ -348,6 +348,8 @@ Stencils build_stencils(double h, const double ctr[3], int nq, const double* xq,
       return (int)((((kx - kx0) * ny) + (ky - ky0)) * 2 + side);
     }
   } G[3];
+  // the three orientations' tables are independent
+#pragma omp parallel for schedule(static, 1)
   for (int o = 0; o < 3; o++) {
     const int a1 = i1s[o], a2 = i2s[o];
     std::vector<long long> key(2 * (size_t)nq);
