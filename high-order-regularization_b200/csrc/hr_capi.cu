@@ -250,6 +250,9 @@ extern "C" void hr_ctx_destroy(hr_ctx* ctx) {
   }
   if (ctx->c.ev_fork) cudaEventDestroy(ctx->c.ev_fork);
   if (ctx->c.ev_join) cudaEventDestroy(ctx->c.ev_join);
+  for (auto& e : ctx->c.pin_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->c.pin) cudaFreeHost(ctx->c.pin);
   delete ctx;
 }
 

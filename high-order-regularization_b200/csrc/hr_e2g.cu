@@ -483,11 +483,11 @@ extern "C" int hr_e2g_get(hr_e2g* E, int which, double* out) {
   if (!E || !out || which < 0 || which > 3) return HR_ERR_ARG;
   Ctx& C = E->owner->c;
   try {
+    HR_CHECK_CUDA(cudaSetDevice(C.device));
     const long M = E->S.N + 1, m3 = M * M * M;
     const double* src = which == 0 ? E->p_bi.p : which == 1 ? E->u_bi.p : which == 2 ? E->p_ext.p : E->u_ext.p;
     long n = (which == 1 || which == 3) ? 3 * m3 : m3;
-    HR_CHECK_CUDA(cudaMemcpyAsync(out, src, sizeof(double) * n, cudaMemcpyDeviceToHost, C.stream));
-    HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
+    d2h_staged(C, out, src, sizeof(double) * n);
   } catch (const hr::Error& e) {
     C.err = e.what();
     return e.code;

@@ -69,6 +69,44 @@ void dev_free(void* p) noexcept {
   }
 }
 
+void d2h_staged(Ctx& C, void* dst, const void* src, size_t bytes) {
+  cudaStream_t st = C.stream;
+  if (bytes <= 2 * kPinChunk) {
+    HR_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    HR_CHECK_CUDA(cudaStreamSynchronize(st));
+    return;
+  }
+  if (!C.pin) {
+    HR_CHECK_CUDA(cudaMallocHost(&C.pin, 2 * kPinChunk));
+    for (auto& e : C.pin_ev) HR_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  char* buf[2] = {static_cast<char*>(C.pin), static_cast<char*>(C.pin) + kPinChunk};
+  const char* s = static_cast<const char*>(src);
+  char* d = static_cast<char*>(dst);
+  const size_t nch = (bytes + kPinChunk - 1) / kPinChunk;
+  auto len = [&](size_t k) { return std::min(kPinChunk, bytes - k * kPinChunk); };
+  auto enqueue = [&](size_t k) {
+    HR_CHECK_CUDA(cudaMemcpyAsync(buf[k & 1], s + k * kPinChunk, len(k), cudaMemcpyDeviceToHost, st));
+    HR_CHECK_CUDA(cudaEventRecord(C.pin_ev[k & 1], st));
+  };
+  enqueue(0);
+  enqueue(1);
+  constexpr size_t kPart = size_t(1) << 20;  // bytes per host thread's piece
+  for (size_t k = 0; k < nch; k++) {
+    HR_CHECK_CUDA(cudaEventSynchronize(C.pin_ev[k & 1]));
+    const size_t n = len(k);
+    char* out = d + k * kPinChunk;
+    const char* in = buf[k & 1];
+    const long nparts = (long)((n + kPart - 1) / kPart);
+#pragma omp parallel for schedule(static)
+    for (long q = 0; q < nparts; q++) {
+      const size_t o = (size_t)q * kPart;
+      std::memcpy(out + o, in + o, std::min(kPart, n - o));
+    }
+    if (k + 2 < nch) enqueue(k + 2);
+  }
+}
+
 void DevTree::build(const hr_surface& S, int P, int N0, double theta, bool direct,
                     cudaStream_t st) {
   HR_REQUIRE(S.n >= 0 && (S.n == 0 || (S.xyz && S.nrml && S.area)), "surface arrays missing");

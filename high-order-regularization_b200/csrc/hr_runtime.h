@@ -94,9 +94,22 @@ struct Ctx {
   int num_sms = 148;
   DBuf<unsigned long long> counters;  // [0] reg pairs [1] plain pairs [2] proxies
   DBuf<int> tc_err;                   // set by a tensor-core kernel whose bounded wait ran out
+  // two pinned host buffers of kPinChunk bytes for staged reads (d2h_staged),
+  // allocated on first use, and the events that mark each one filled
+  void* pin = nullptr;
+  cudaEvent_t pin_ev[2] = {nullptr, nullptr};
   // throws if a tensor-core kernel of this context reported a timed-out wait
   void check_tc();
 };
+
+// Bytes of one pinned staging buffer of d2h_staged.
+constexpr size_t kPinChunk = size_t(16) << 20;
+
+// Reads `bytes` from device memory into (pageable) host memory through the
+// context's two pinned buffers: the copy of chunk k + 1 runs while host threads
+// move chunk k into place. Returns when all of it has arrived. Reads of up to
+// two chunks go straight to `dst`.
+void d2h_staged(Ctx& C, void* dst, const void* src, size_t bytes);
 
 // A surface on the device: sources in tree order, its tree, density buffers
 // and the upward-pass work items.
