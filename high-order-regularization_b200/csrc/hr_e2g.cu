@@ -368,21 +368,22 @@ extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
     e2g_batch(*E, HR_FP64, C);  // the reduced-precision batches are built on first use
     E->pairs = 2LL * (E->nface + E->nband) * (long long)surf.n;
     // masks: BAND2 points, and exterior points outside BAND2 (E2G/main.cpp:1611-1614, 1654-1672)
-    std::vector<uint8_t> b2((size_t)M * M * M, 0), om((size_t)M * M * M, 0);
+    std::vector<uint8_t, e2g_setup::NoInitAlloc<uint8_t>> b2((size_t)M * M * M), om((size_t)M * M * M);
 #pragma omp parallel for schedule(static)
     for (int i = 0; i < M; i++)
       for (int j = 0; j < M; j++)
         for (int k = 0; k < M; k++) {
           long g = ((long)i * M + j) * M + k;
           int ind = S.nrst[g];
-          if (ind != -1 && S.band2[ind]) b2[g] = 1;
+          const bool in2 = ind != -1 && S.band2[ind];
+          b2[g] = in2 ? 1 : 0;
           double x[3] = {i * h, j * h, k * h};
           double u0 = x[0] - 1.5, u1 = x[1] - 1.5, u2 = x[2] - 1.5;
           double levl = u0 * u0 / 1.0 + u1 * u1 / 0.25 + u2 * u2 / 0.25 - 1.0;
-          if (levl > 0 && (ind == -1 || !S.band2[ind])) om[g] = 1;
+          om[g] = (levl > 0 && !in2) ? 1 : 0;
         }
-    E->mband2.upload(b2, st);
-    E->mout.upload(om, st);
+    E->mband2.upload(b2.data(), b2.size(), st);
+    E->mout.upload(om.data(), om.size(), st);
     size_t m3 = (size_t)M * M * M;
     E->p_bi.alloc(m3);
     E->u_bi.alloc(3 * m3);

@@ -320,6 +320,9 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
     const int P1 = T.P + 1;
     const double Pf = (double)P1 * P1 * P1;
     per[t].resize(L.nblocks());
+    // blocks are independent; every cost is a multiple of 1/2 far below 2^52,
+    // so the sum is exact (and the item size the same) in any order
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : total)
     for (int b = 0; b < L.nblocks(); b++) {
       for (int e = L.blk_start[b]; e < L.blk_start[b + 1]; e++) {
         const Entry& E = L.entries[e];

@@ -13,6 +13,7 @@
 // k"; the same numbering is produced here with a parallel first-claim pass.
 #include <algorithm>
 #include <atomic>
+#include <memory>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -302,8 +303,10 @@ void build(Scene& S, int N, double band1, double band2) {
   for (int j = 0; j < nq; j++) stokeslet_density(&S.xq[3 * j], &S.f[3 * j]);
   // band tagging: first quadrature point (in order) within (BAND1+1)h of a grid point
   const long M = N + 1;
-  std::vector<std::atomic<int>> claim(M * M * M);
-  for (auto& c : claim) c.store(nq, std::memory_order_relaxed);
+  // (C++17: new std::atomic<int>[] leaves the values for the parallel fill)
+  std::unique_ptr<std::atomic<int>[]> claim(new std::atomic<int>[M * M * M]);
+#pragma omp parallel for schedule(static)
+  for (long g = 0; g < M * M * M; g++) claim[g].store(nq, std::memory_order_relaxed);
   const double tol = 1.e-12;
   const int width = (int)ceil(band1);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -332,9 +335,25 @@ void build(Scene& S, int N, double band1, double band2) {
     long g;
     double b, x0[3], n0[3];
   };
+  // claimed grid points in grid order: counted per i-plane, then filled
   std::vector<long> cand;
-  for (long g = 0; g < M * M * M; g++)
-    if (claim[g].load(std::memory_order_relaxed) < nq) cand.push_back(g);
+  {
+    std::vector<long> cnt(M + 1, 0);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < M; i++) {
+      long c = 0;
+      for (long g = i * M * M; g < (i + 1) * M * M; g++) c += claim[g].load(std::memory_order_relaxed) < nq;
+      cnt[i + 1] = c;
+    }
+    for (long i = 0; i < M; i++) cnt[i + 1] += cnt[i];
+    cand.resize(cnt[M]);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < M; i++) {
+      long o = cnt[i];
+      for (long g = i * M * M; g < (i + 1) * M * M; g++)
+        if (claim[g].load(std::memory_order_relaxed) < nq) cand[o++] = g;
+    }
+  }
   // quadrature points bucketed by grid cell (dense CSR table over the cells
   // the surface occupies, ascending point index per cell), for the retries below
   long cmin[3] = {0, 0, 0}, cmax[3] = {-1, -1, -1};
@@ -418,7 +437,9 @@ void build(Scene& S, int N, double band1, double band2) {
   std::vector<Tag> kept(nkept);
   for (size_t c = 0; c < cand.size(); c++)
     if (ok[c]) kept[qstart[tags[c].q]++] = tags[c];
-  S.nrst.assign(M * M * M, -1);
+  S.nrst.resize(M * M * M);
+#pragma omp parallel for schedule(static)
+  for (long g = 0; g < M * M * M; g++) S.nrst[g] = -1;
   S.b.resize(nkept);
   S.x0.resize(3 * nkept);
   S.n0.resize(3 * nkept);
