@@ -347,43 +347,63 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
   //    total / (SMs x 4 resident CTAs x 16 waves), never below two tiles;
   //    small items keep the tail short where the cost estimate is off.
   const double target = std::max(total / (num_sms * 4.0 * 16.0), 2.0 * 256.0 * 2.0);
-  std::vector<Seg> segs;
-  std::vector<std::pair<double, BlockRef>> items;
+  // Blocks in task order; each block's runs are formed on its own (in
+  // parallel), then offsets give every segment and item (slot) the position
+  // a serial pass over the blocks would give it.
+  std::vector<int2> tblocks;
+  for (size_t t = 0; t < tasks.size(); t++)
+    for (int b = 0; b < (int)per[t].size(); b++) tblocks.push_back(make_int2((int)t, b));
+  const long nbt = (long)tblocks.size();
+  std::vector<std::vector<std::pair<int, double>>> runs(nbt);  // per block: (segments, cost) per item
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long q = 0; q < nbt; q++) {
+    const auto& v = per[tblocks[q].x][tblocks[q].y];
+    size_t i = 0;
+    while (i < v.size()) {
+      double c = 0.0;
+      int n = 0;
+      do {
+        c += v[i].cost;
+        i++;
+        n++;
+      } while (i < v.size() && c + v[i].cost <= target);
+      runs[q].push_back({n, c});
+    }
+    // a block without work still gets one (empty) item so that its partial
+    // slot is written
+    if (v.empty()) runs[q].push_back({0, 0.0});
+  }
+  std::vector<long> seg_off(nbt + 1, 0), slot_off(nbt + 1, 0);
+  for (long q = 0; q < nbt; q++) {
+    seg_off[q + 1] = seg_off[q] + (long)per[tblocks[q].x][tblocks[q].y].size();
+    slot_off[q + 1] = slot_off[q] + (long)runs[q].size();
+  }
+  HR_REQUIRE(seg_off[nbt] < (1L << 31) && slot_off[nbt] < (1L << 31), "batch too large for 32-bit segment indices");
+  std::vector<Seg> segs(seg_off[nbt]);
+  std::vector<std::pair<double, BlockRef>> items(slot_off[nbt]);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long q = 0; q < nbt; q++) {
+    const int t = tblocks[q].x, b = tblocks[q].y;
+    const auto& v = per[t][b];
+    int sg = (int)seg_off[q], it = (int)slot_off[q];
+    size_t i = 0;
+    for (const auto& r : runs[q]) {
+      BlockRef ref{t, b, sg, sg + r.first, it};
+      for (int k = 0; k < r.first; k++) segs[sg++] = v[i++].s;
+      items[it++] = {r.second, ref};
+    }
+  }
+  // per task: the slot of each block's first item, then the task's end
   std::vector<int> starts;
   std::vector<size_t> start_off(tasks.size());
-  std::vector<int2> tblocks;
-  int slot = 0;
-  for (size_t t = 0; t < tasks.size(); t++) {
-    start_off[t] = starts.size();
-    const int nb = (int)per[t].size();
-    for (int b = 0; b < nb; b++) {
-      starts.push_back(slot);
-      tblocks.push_back(make_int2((int)t, b));
-      const auto& v = per[t][b];
-      size_t i = 0;
-      while (i < v.size()) {
-        BlockRef it;
-        it.task = (int)t;
-        it.blk = b;
-        it.seg0 = (int)segs.size();
-        double c = 0.0;
-        do {
-          segs.push_back(v[i].s);
-          c += v[i].cost;
-          i++;
-        } while (i < v.size() && c + v[i].cost <= target);
-        it.seg1 = (int)segs.size();
-        it.slot = slot++;
-        items.push_back({c, it});
-      }
-      if (v.empty()) {
-        // a block without work still gets one (empty) item so that its
-        // partial slot is written
-        BlockRef it{(int)t, b, (int)segs.size(), (int)segs.size(), slot++};
-        items.push_back({0.0, it});
-      }
+  int slot = (int)slot_off[nbt];
+  {
+    long q = 0;
+    for (size_t t = 0; t < tasks.size(); t++) {
+      start_off[t] = starts.size();
+      for (int b = 0; b < (int)per[t].size(); b++, q++) starts.push_back((int)slot_off[q]);
+      starts.push_back((int)slot_off[q]);
     }
-    starts.push_back(slot);
   }
   // lean items first (their own launch: on-surface kinds, or the extend-to-grid
   // box-face sums), each part by decreasing cost
