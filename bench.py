@@ -232,6 +232,16 @@ def warm_guess_fn(ctx, geo, dev):
     return fn, feat_s
 
 
+def fp64_true_residual(plan, b, x):
+    """||b - A x|| / ||b|| with the plan's FP64 operator (outside any timed region)."""
+    import torch
+
+    y = torch.empty_like(x)
+    plan.matvec_dev(x, y)
+    torch.cuda.synchronize()
+    return float(torch.linalg.vector_norm(b - y) / torch.linalg.vector_norm(b))
+
+
 def timed_solves(plan, stream, flush, f1, f2, b, x, prec, steps, guess=None):
     """steps x (L2 flush; RHS + optional guess + GMRES), CUDA events on the plan's stream."""
     import torch
@@ -252,10 +262,86 @@ def timed_solves(plan, stream, flush, f1, f2, b, x, prec, steps, guess=None):
         times.append(e0.elapsed_time(e1))
         reps.append(rep)
     r = reps[-1]
+    # the plain FP64 solve stops on GMRES's recurrence residual; its FP64 true
+    # residual is computed here, after the timed steps (the reduced-precision
+    # solves compute theirs inside, as their stopping test)
+    true_res = r["true_residual"] if r["true_residual"] >= 0.0 else fp64_true_residual(plan, b, x)
     return {"ms_per_step": sum(times) / len(times), "ms_min": min(times), "ms_max": max(times),
             "gmres_iterations": r["iterations"],
             "matvecs_fp64": r["matvecs_fp64"], "matvecs_mixed": r["matvecs_mixed"], "residual": r["residual"],
-            "true_residual": r["true_residual"], "guess_rejected": r["guess_rejected"]}
+            "true_residual": true_res, "guess_rejected": r["guess_rejected"]}
+
+
+def solve_variants(ctx, plan, geo, dev, steps, inner, with_warm=True):
+    """The metric's comparison on one plan, each variant after one untimed
+    solve (the reduced-precision batches are built on first use): plain FP64,
+    mixed precision (GMRES-IR on the plan's treecode), mixed + learned warm
+    start and, with an inner treecode (P, N0), mixed and mixed + warm start
+    with the inner cycles on it (the FP64 true residuals keep the plan's
+    treecode)."""
+    import torch
+
+    import highreg
+
+    n = plan.n
+    f1 = torch.tensor(geo["f0"], dtype=torch.float64, device=dev)
+    f2 = torch.tensor(geo["f1"], dtype=torch.float64, device=dev)
+    b = torch.zeros(n, dtype=torch.float64, device=dev)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    stream = torch.cuda.ExternalStream(plan.stream(), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    variants = {}
+    names = (("fp64", highreg.HR_FP64), ("mixed", highreg.HR_MIXED)) if inner is None else (("fp64", highreg.HR_FP64),)
+    for name, pr in names:
+        timed_solves(plan, stream, flush, f1, f2, b, x, pr, 1)
+        variants[name] = timed_solves(plan, stream, flush, f1, f2, b, x, pr, steps)
+    guess, feat_s = warm_guess_fn(ctx, geo, dev) if with_warm else (None, None)
+    if guess is not None and inner is None:
+        timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, guess)
+        v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, steps, guess)
+        v["features_host_ms"] = 1e3 * feat_s
+        variants["mixed_warm"] = v
+    ms_dl_inner = None
+    if inner is not None:
+        inner_err = plan.set_inner_tree(inner[0], inner[1], THETA)
+        for name, g in (("mixed_inner", None), ("mixed_inner_warm", guess)):
+            if name.endswith("warm") and g is None:
+                continue
+            timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, g)
+            v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, steps, g)
+            v["inner_tree"] = {"P": inner[0], "N0": inner[1], "theta": THETA, "rel_l2_error": inner_err}
+            if g is not None:
+                v["features_host_ms"] = 1e3 * feat_s
+            variants[name] = v
+        plan.matvec_dev(x, b, highreg.HR_MIXED)
+        ms_dl_inner = plan.time_batch(3, 10)
+        plan.set_inner_tree(0, 0, THETA)
+    for v in variants.values():
+        v["speedup_vs_fp64"] = variants["fp64"]["ms_per_step"] / v["ms_per_step"]
+    del guess  # releases the network before the context goes
+    torch.cuda.synchronize()
+    return variants, ms_dl_inner
+
+
+def run_h256_block(ctx, dev, steps):
+    """The precision study's configuration, timed in the same run: the
+    two-surface solve at h = 1/256 (n = 2,740,992), KITC P = 10, N0 = 8000,
+    GMRES(50) to 1e-10; plain FP64 against mixed precision with the inner
+    treecode P = 5, N0 = 2000 (and with the learned warm start)."""
+    import highreg
+
+    t0 = time.perf_counter()
+    geo = highreg.Geometry2S(256).scene
+    plan = highreg.Plan2S(ctx, geo, mode=highreg.HR_TREE, P=10, N0=8000, theta=THETA)
+    setup_s = time.perf_counter() - t0
+    variants, ms_inner = solve_variants(ctx, plan, geo, dev, steps, (5, 2000))
+    out = {"workload": "two-surface solve h=1/256 (n=%d), KITC P=10 N0=8000 theta=0.6, GMRES restart 50 tol 1e-10"
+                       % plan.n,
+           "steps": steps, "setup_seconds": setup_s, "variants": variants,
+           "ms_per_launch_mixed_inner_tree": ms_inner,
+           "target": "mixed + learned warm start >= 3x plain FP64"}
+    plan.close()
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -311,35 +397,8 @@ def run_ours(args, rank, world, local_rank):
 
     # the metric's comparison on the same workload and protocol: plain FP64,
     # mixed precision, and mixed precision with the learned warm start
-    variants = {}
-    for name, pr in (("fp64", highreg.HR_FP64), ("mixed", highreg.HR_MIXED)):
-        # one untimed solve first: the reduced-precision batches are built on first use
-        timed_solves(plan, stream, flush, f1, f2, b, x, pr, 1)
-        variants[name] = timed_solves(plan, stream, flush, f1, f2, b, x, pr, args.steps)
-    guess, feat_s = warm_guess_fn(ctx, geo, dev)
-    if guess is not None:
-        timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, guess)
-        v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, args.steps, guess)
-        v["features_host_ms"] = 1e3 * feat_s
-        variants["mixed_warm"] = v
-    # GMRES-IR with the inner cycles on a treecode of their own (lower degree
-    # and leaf size); the FP64 true residuals keep the benchmark's treecode
-    ms_dl_inner = None
-    if INNER is not None:
-        inner_err = plan.set_inner_tree(INNER[0], INNER[1], THETA)
-        for name, g in (("mixed_inner", None), ("mixed_inner_warm", guess)):
-            if name.endswith("warm") and g is None:
-                continue
-            timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, 1, g)
-            v = timed_solves(plan, stream, flush, f1, f2, b, x, highreg.HR_MIXED, args.steps, g)
-            v["inner_tree"] = {"P": INNER[0], "N0": INNER[1], "theta": THETA, "rel_l2_error": inner_err}
-            variants[name] = v
-        plan.matvec_dev(x, b, highreg.HR_MIXED)
-        ms_dl_inner = plan.time_batch(3, 20)
-        plan.set_inner_tree(0, 0, THETA)
-    for v in variants.values():
-        v["speedup_vs_fp64"] = variants["fp64"]["ms_per_step"] / v["ms_per_step"]
-    del guess  # releases the network before the context goes
+    true_res_main = fp64_true_residual(plan, b, x) if prec == highreg.HR_FP64 else reps[-1]["true_residual"]
+    variants, ms_dl_inner = solve_variants(ctx, plan, geo, dev, args.steps, INNER)
     t_local = sum(times) / 1e3
     it = reps[-1]["iterations"]
     mv_per_step = reps[-1]["matvecs_fp64"] + reps[-1]["matvecs_mixed"]
@@ -367,8 +426,8 @@ def run_ours(args, rank, world, local_rank):
                 "peak_fp32": peak32 / 1e12}
     if H_INV == 64 and P == 6 and N0 == 2000:
         # dram__bytes_read.sum + dram__bytes_write.sum of this launch from one ncu capture
-        # (profiles/eval_kernel_fp64_stresslet_h64.md): sources are staged once per tile, so
-        # DRAM traffic is tiny next to the compute; the bound is the FP64 pipe
+        # of both kernels of the batch at this workload: sources are staged once per tile,
+        # so DRAM traffic is tiny next to the compute; the bound is the FP64 pipe
         roofline["traffic"] = 10836992 + 157952 + 10935808 + 0
         roofline["traffic_source"] = "ncu capture of this kernel at this workload"
 
@@ -399,6 +458,11 @@ def run_ours(args, rank, world, local_rank):
            "note": "scene upload and plan (trees, interaction lists, stencils on the host) + RHS + solve + "
                    "solution read back, through the C ABI with host buffers"}
 
+    # the precision study's h = 1/256 comparison, timed in the same run
+    h256 = None
+    if world == 1 and H_INV == 64 and not args.no_h256:
+        h256 = run_h256_block(ctx, dev, args.h256_steps)
+
     line = None
     if rank == 0:
         cpu = None
@@ -422,9 +486,9 @@ def run_ours(args, rank, world, local_rank):
                            "l2": "flushed (256 MB write) before each timed step",
                            "gmres_iterations": it, "matvecs_per_step": mv_per_step,
                            "pairs_per_step": pairs_step, "solve_seconds": t_max / args.steps,
-                           "final_residual": reps[-1]["residual"], "true_residual": reps[-1]["true_residual"],
+                           "final_residual": reps[-1]["residual"], "true_residual": true_res_main,
                            "precision": args.precision, "work_matvec": w_mv, "work_rhs": w_rhs,
-                           "variants": variants},
+                           "variants": variants, "h256": h256},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
                 "gpu_launches": launches}
         print(json.dumps(line))
@@ -536,6 +600,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-h256", action="store_true",
+                    help="skip the h = 1/256 FP64 / mixed / warm-start comparison of the default run")
+    ap.add_argument("--h256-steps", type=int, default=2, help="timed solves per variant in the h = 1/256 block")
     ap.add_argument("--h", type=int, default=64, help="1/h of the workload (64 is the benchmark)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--P", type=int, default=6, help="treecode degree (6 with h=1/64; 10 with h=1/256)")

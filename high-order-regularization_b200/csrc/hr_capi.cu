@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <exception>
 #include <random>
 #include <thread>
@@ -463,6 +464,7 @@ struct hr_plan2s {
   // batch), its uploads on a stream of its own; every other use of the plan
   // first waits for it (plan_ready).
   std::thread dl_thread;
+  std::mutex dl_mu;  // one joiner, if two host threads reach plan_ready at once
   std::exception_ptr dl_error;
   cudaStream_t up = nullptr;
   cudaEvent_t up_done = nullptr;
@@ -566,6 +568,7 @@ void plan_batches(hr_plan2s& P) {
 // Waits for the FP64 stresslet batch of plan_batches (and orders the plan's
 // stream after its uploads); rethrows its error on every use.
 void plan_ready(hr_plan2s& P) {
+  std::lock_guard<std::mutex> lock(P.dl_mu);
   if (P.dl_thread.joinable()) {
     P.dl_thread.join();
     if (!P.dl_error) HR_CHECK_CUDA(cudaStreamWaitEvent(P.C->stream, P.up_done, 0));

@@ -11,7 +11,9 @@
 //
 // Set-up: the first call on a device (with that device current) looks up the
 // array's device address with cudaGetSymbolAddress and caches it for that
-// device; make that first call before any stream capture. Every call shares
+// device; make that first call before any stream capture. The cached address
+// belongs to the device's primary context: after cudaDeviceReset on that
+// device the entry point must not be called again in this process. Every call shares
 // the array and leaves the last call's partial sums in it; each call writes
 // every slot it later reads, so nothing needs clearing, but two calls that
 // overlap on the GPU (different streams, no ordering) race on the array.
@@ -112,6 +114,8 @@ extern "C" int hr_stokeslet_away_noalloc(const double* xyz_src_dev, const double
                                          const double* f_dev, int nq, const double* xyz_tgt_dev,
                                          int nt, double* out_dev, void* stream) {
   if (nq < 0 || nt < 0) return HR_ERR_ARG;
+  // interleaved source and target indices (3 j + k) are int arithmetic
+  if (3LL * nq > 2147483647LL) return HR_ERR_ARG;
   if (nt == 0) return HR_OK;
   if ((long long)3 * nt > kScratchDoubles) return HR_ERR_ARG;  // beyond the scratch array
   if (!xyz_tgt_dev || !out_dev || (nq > 0 && (!xyz_src_dev || !area_dev || !f_dev))) return HR_ERR_ARG;
@@ -138,6 +142,8 @@ extern "C" int hr_stokeslet_away_noalloc(const double* xyz_src_dev, const double
   away_partial_kernel<<<grid, kThreads, 0, st>>>(xyz_src_dev, area_dev, f_dev, nq, xyz_tgt_dev, nt,
                                                  chunk, scratch);
   away_reduce_kernel<<<(nt + 255) / 256, 256, 0, st>>>(scratch, nt, nchunks, scale, out_dev);
-  if (cudaGetLastError() != cudaSuccess) return HR_ERR_CUDA;
+  // peek, not get: a launch error stays visible to the caller's own error
+  // handling, and an earlier error of the caller's is not consumed here
+  if (cudaPeekAtLastError() != cudaSuccess) return HR_ERR_CUDA;
   return HR_OK;
 }

@@ -409,6 +409,10 @@ int hr_measure_fp32_peak(hr_ctx* ctx, double* flops_per_s);
  * the array up once; make it before any stream capture. All calls share the
  * array and leave their partial sums in it; every slot read is written
  * first, so nothing needs clearing, but calls that overlap on the GPU race.
+ * The looked-up address belongs to the device's primary context: do not call
+ * this again after cudaDeviceReset on that device. Launch errors are reported
+ * with cudaPeekAtLastError (the thread's last error is left as it is). nq
+ * above 715,827,882 returns HR_ERR_ARG (int source indices).
  * Enqueued on `stream` (a cudaStream_t, NULL = legacy default stream). */
 int hr_stokeslet_away_noalloc(const double* xyz_src_dev, const double* area_dev, const double* f_dev, int nq,
                               const double* xyz_tgt_dev, int nt, double* out_dev, void* stream);

@@ -31,8 +31,22 @@ import sys
 import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_ROOT = os.environ.get("HR_REFERENCE_ROOT", "/root/reference")
 REF_OUT = os.path.join(HERE, "_ref")
+
+
+def reference_root(path: str | None = None) -> str | None:
+    """The reference source tree: ``path`` if given, else $HR_REFERENCE_ROOT,
+    else a directory named ``reference`` beside this repository's root. An
+    explicitly named tree that does not exist is an error; the default one may
+    be absent (machines that only run the prebuilt files), and then None."""
+    explicit = path or os.environ.get("HR_REFERENCE_ROOT")
+    if explicit:
+        if not os.path.isdir(os.path.join(explicit, "highreg_stokes_2surf")):
+            raise FileNotFoundError("reference tree not found at %s (HR_REFERENCE_ROOT / argument)" % explicit)
+        return explicit
+    default = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+    return default if os.path.isdir(os.path.join(default, "highreg_stokes_2surf")) else None
+
 
 # (P, N0) treecode variants of the reference two-surface program.
 KITC_VARIANTS = [(6, 1000), (6, 2000), (4, 300), (10, 8000), (8, 4000)]
@@ -66,13 +80,16 @@ def ref2s_lib_name(P: int, N0: int) -> str:
     return os.path.join(REF_OUT, "libref2s_P%d_N%d.so" % (P, N0))
 
 
-def build_reference(force: bool = False) -> list:
+def build_reference(force: bool = False, root: str | None = None) -> list:
     """Compile the reference programs; returns the list of built libraries.
 
-    Does nothing (returns []) when the reference tree is not present.
+    Does nothing (returns []) when no reference tree is found.
     """
-    s2 = os.path.join(REF_ROOT, "highreg_stokes_2surf")
-    e2g = os.path.join(REF_ROOT, "highreg_stokes_extend_to_grid")
+    root = reference_root(root)
+    if root is None:
+        return []
+    s2 = os.path.join(root, "highreg_stokes_2surf")
+    e2g = os.path.join(root, "highreg_stokes_extend_to_grid")
     if not (os.path.isdir(s2) and os.path.isdir(e2g)):
         return []
     os.makedirs(REF_OUT, exist_ok=True)
@@ -116,13 +133,16 @@ def build_reference(force: bool = False) -> list:
     return built
 
 
-def build_relinked_reference(force: bool = False):
+def build_relinked_reference(force: bool = False, root: str | None = None):
     """The reference's unmodified two-surface driver (main.cpp, surface.cpp,
     utilities.cpp) linked against the product's reference-signature layer
     (libhighreg_refapi.so) instead of its own KITC.cpp / stokeslets.cpp /
     stresslets.cpp: the drop-in test of the C++ boundary. Needs the reference
     tree and the built product library; returns the binary path or None."""
-    s2 = os.path.join(REF_ROOT, "highreg_stokes_2surf")
+    root = reference_root(root)
+    if root is None:
+        return None
+    s2 = os.path.join(root, "highreg_stokes_2surf")
     pkg = os.path.join(os.path.dirname(HERE), "high-order-regularization_b200")
     lib = os.path.join(pkg, "libhighreg_refapi.so")
     if not os.path.isdir(s2) or not os.path.exists(lib):

@@ -329,6 +329,34 @@ class Ref2S:
         k = self.lib.ref2s_solve(_d(x), _d(r), 400)
         return x, r[:k]
 
+    def load(self, geo: dict, g=None):
+        """Loads a scene in the checker's dict layout (see Oracle.scene) into
+        the reference program instead of its own set-up; g (optional, per
+        surface) is the stresslet density."""
+        for s in (0, 1):
+            n = len(geo["area%d" % s])
+            gs = np.zeros(3 * n) if g is None else _f64(g[s])
+            self.lib.ref2s_load(s, n, _d(_f64(geo["xq%d" % s])), _d(_f64(geo["nrm%d" % s])),
+                                _d(_f64(geo["area%d" % s])), _d(_f64(geo["f%d" % s])), _d(gs),
+                                _d(_f64(geo["b%d" % s])), _d(_f64(geo["x0%d" % s])), _d(_f64(geo["n0%d" % s])),
+                                _d(_f64(geo["f0%d" % s])), _i(np.ascontiguousarray(geo["nrst%d" % s], np.int32)),
+                                _i(np.ascontiguousarray(geo["i123%d" % s], np.int32)), ctypes.c_double(geo["h"]),
+                                ctypes.c_double(geo["DEL"]))
+        self.nq = tuple(len(geo["area%d" % s]) for s in (0, 1))
+        self.h, self.DEL = float(geo["h"]), float(geo["DEL"])
+        return self
+
+    def sample_eval(self, kind, s, t, idx):
+        """Direct sums (kind 0 Stokeslet of f, 1 stresslet of g) of surface s
+        at the sampled targets idx of set t, by the reference's own functions;
+        returns (out (3 per target), g0 at the targets' nearest points (the
+        stresslet off the surface only, else None))."""
+        idx = np.ascontiguousarray(idx, np.int32)
+        out = np.zeros(3 * len(idx))
+        g0 = np.zeros(3 * len(idx)) if (kind == 1 and s != t) else None
+        self.lib.ref2s_sample_eval(kind, s, t, len(idx), _i(idx), _d(out), _d(g0))
+        return out, g0
+
     def geometry(self):
         """Scene geometry in the checker's dict layout (see Oracle.scene)."""
         ctrs = [(0.0, 0.0, -0.5 - 1.0 / 4096.0), (0.0, 0.0, 0.5)]
@@ -420,6 +448,33 @@ class RefE2G:
     def run(self):
         self.lib.refe2g_run()
         return self.log()
+
+    def load(self, N, scene):
+        """Loads an extend-to-grid scene (the dict of the product's
+        E2G.scene(): quadrature, density, tagged targets, index grid)
+        instead of the reference's own set-up."""
+        self.N = N
+        nq, nt = len(scene["area"]), len(scene["b"])
+        self.lib.refe2g_load(N, nq, _d(_f64(scene["xq"])), _d(_f64(scene["nrm"])), _d(_f64(scene["area"])),
+                             _d(_f64(scene["f"])), nt, _d(_f64(scene["b"])), _d(_f64(scene["x0"])),
+                             _d(_f64(scene["n0"])), _i(np.ascontiguousarray(scene["band2"], np.int32)),
+                             _i(np.ascontiguousarray(scene["nrst"], np.int32)))
+        self.nq, self.nt = nq, nt
+        h = 3.0 / N
+        self.h = h
+        return self
+
+    def set_nrst(self, nrst_grid):
+        self.lib.refe2g_set_nrst(_i(np.ascontiguousarray(nrst_grid, np.int32)))
+
+    def away_points(self, xyz):
+        """The reference's plain Stokeslet and pressure sums at points xyz
+        (3 per point): returns (u (3 per point), p)."""
+        xyz = _f64(xyz)
+        n = len(xyz) // 3
+        u, p = np.zeros(3 * n), np.zeros(n)
+        self.lib.refe2g_away_points(n, _d(xyz), _d(u), _d(p))
+        return u, p
 
     def p_exact(self, x, y, z):
         return self.lib.refe2g_p_exact(ctypes.c_double(x), ctypes.c_double(y), ctypes.c_double(z))

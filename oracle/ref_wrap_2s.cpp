@@ -252,6 +252,96 @@ int ref2s_solve(double* x_out, double* resid, int max_resid) {
   return count;
 }
 
+// Loads surface s and target set s from arrays instead of building them (the
+// reference's own set-up scans every quadrature point per target and takes
+// hours at h = 1/256). Layouts as in ref2s_get_surface / ref2s_get_targets;
+// the target set s holds surface s's quadrature points with nearest data on
+// the other surface. h and delta are the scene's.
+void ref2s_load(int s, int n, const double* xyz, const double* nrml, const double* area,
+                const double* f, const double* g, const double* b, const double* x0,
+                const double* n0, const double* f0, const int* nrst_idx, const int* i123,
+                double h, double delta) {
+  g_h = h;
+  g_DEL = delta;
+  g_N = (int)lround(1.0 / h);
+  S[s].assign(n, Surf_point());
+  T[s].assign(n, Target_point());
+  for (int i = 0; i < n; i++) {
+    for (int k = 0; k < 3; k++) {
+      S[s][i].x[k] = xyz[3 * i + k];
+      S[s][i].Nrml[k] = nrml[3 * i + k];
+      S[s][i].f[k] = f[3 * i + k];
+      S[s][i].g[k] = g[3 * i + k];
+      T[s][i].nrst_Nrml[k] = n0[3 * i + k];
+      T[s][i].nrst_f[k] = f0[3 * i + k];
+    }
+    S[s][i].Area = area[i];
+    T[s][i].x = xyz[3 * i];
+    T[s][i].y = xyz[3 * i + 1];
+    T[s][i].z = xyz[3 * i + 2];
+    T[s][i].b = b[i];
+    T[s][i].nrst_x = x0[3 * i];
+    T[s][i].nrst_y = x0[3 * i + 1];
+    T[s][i].nrst_z = x0[3 * i + 2];
+    T[s][i].nrst = nrst_idx[i];
+    T[s][i].i1 = i123[3 * i];
+    T[s][i].i2 = i123[3 * i + 1];
+    T[s][i].i3 = i123[3 * i + 2];
+  }
+}
+
+// Direct (use_tree = 0) boundary sums of surface s's density at a sample of
+// target set t, through the reference's own functions:
+//   kind 0 Stokeslet, kind 1 stresslet;
+//   s != t: eval_Stokes_SL_offSurf / eval_Stokes_DL_offSurf
+//     (2S/stokeslets.cpp:12-86, 2S/stresslets.cpp:13-96) on the sampled
+//     targets; for the stresslet, interpolate_DL_density (2S/main.cpp:916-1046)
+//     first fills their nearest-point densities g0 (also written to g0_out);
+//   s == t: the per-target on-surface sums stokes_SL_7ord_onSurf /
+//     stokes_DL_7ord_onSurf (2S/stokeslets.cpp:188-225,
+//     2S/stresslets.cpp:236-279) with the subtraction data the drivers
+//     eval_Stokes_*_onSurf take from Surfc[i] (2S/stokeslets.cpp:167,
+//     2S/stresslets.cpp:215-217).
+void ref2s_sample_eval(int kind, int s, int t, int n, const int* idx, double* out, double* g0_out) {
+  CoutCapture cap;
+  int nq = (int)S[s].size();
+  if (s != t) {
+    vector<Target_point> sub(n);
+    for (int i = 0; i < n; i++) sub[i] = T[t][idx[i]];
+    vector<double> res(3 * n, 0.0);
+    if (kind == 0) {
+      eval_Stokes_SL_offSurf(g_h, g_DEL, nq, S[s], n, sub, res);
+    } else {
+      interpolate_DL_density(s + 1, g_h, nq, S[s], n, sub);
+      if (g0_out)
+        for (int i = 0; i < n; i++)
+          for (int k = 0; k < 3; k++) g0_out[3 * i + k] = sub[i].nrst_g[k];
+      eval_Stokes_DL_offSurf(g_h, g_DEL, nq, S[s], n, sub, res);
+    }
+    memcpy(out, res.data(), sizeof(double) * 3 * n);
+    return;
+  }
+  vector<double> q(3 * nq);
+  for (int j = 0; j < nq; j++)
+    for (int k = 0; k < 3; k++) q[3 * j + k] = kind == 0 ? S[s][j].f[k] : S[s][j].g[k];
+#pragma omp parallel
+  {
+    vector<double> res(3, 0.0);
+#pragma omp for schedule(dynamic, 4)
+    for (int m = 0; m < n; m++) {
+      const int i = idx[m];
+      const Surf_point& P = S[s][i];
+      if (kind == 0) {
+        double f0_dot_n0 = dot_product(P.f, P.Nrml);
+        stokes_SL_7ord_onSurf(g_DEL, nq, S[s], q, f0_dot_n0, P.x[0], P.x[1], P.x[2], res);
+      } else {
+        stokes_DL_7ord_onSurf(g_DEL, nq, S[s], q, P.g, P.x[0], P.x[1], P.x[2], res);
+      }
+      for (int k = 0; k < 3; k++) out[3 * m + k] = res[k];
+    }
+  }
+}
+
 // Scalar kernels for kernel-level checks (2S/utilities.cpp:163-337).
 void ref2s_reg_coeff(double lam, double* c) { get_reg_coeff_7ord(lam, c[0], c[1], c[2]); }
 void ref2s_sl_7ord(double r, double d, const double* c, double* s) {

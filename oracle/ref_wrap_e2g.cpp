@@ -218,6 +218,64 @@ void refe2g_run(void) {
   test_Stokes_Poisson3d_FD(g_L, g_N, g_h, g_DEL);
 }
 
+// Loads a scene from arrays instead of building it (the reference's own
+// set-up at N = 384 takes minutes of serial work): quadrature points, the
+// density, the tagged targets and the (N+1)^3 nearest-point index grid, in
+// the layouts of refe2g_get_surface / refe2g_get_targets / refe2g_get_nrst.
+void refe2g_load(int N, int nq, const double* xyz, const double* nrml, const double* area,
+                 const double* f, int nt, const double* b, const double* x0, const double* n0,
+                 const int* band2, const int* nrst_grid) {
+  if (nrst) free3(nrst, g_N);
+  g_N = N;
+  g_L = 3.0;
+  g_h = g_L / N;
+  double kappa0 = 4.0, q = 5.0 / 7.0;
+  double kappa = kappa0 * pow(1.0 / 64.0, 1.0 - q);
+  g_DEL = kappa * pow(g_h, q);
+  Surfc.assign(nq, Surf_point());
+  f_ex.assign(f, f + 3 * (size_t)nq);
+  for (int i = 0; i < nq; i++) {
+    for (int k = 0; k < 3; k++) {
+      Surfc[i].x[k] = xyz[3 * i + k];
+      Surfc[i].Nrml[k] = nrml[3 * i + k];
+    }
+    Surfc[i].Area = area[i];
+  }
+  Target.assign(nt, Target_point());
+  for (int i = 0; i < nt; i++) {
+    Target[i].b = b[i];
+    Target[i].nrst_x = x0[3 * i];
+    Target[i].nrst_y = x0[3 * i + 1];
+    Target[i].nrst_z = x0[3 * i + 2];
+    for (int k = 0; k < 3; k++) Target[i].nrst_Nrml[k] = n0[3 * i + k];
+    Target[i].band2 = band2[i] != 0;
+  }
+  nrst = alloc3<int>(N);
+  to3(nrst_grid, nrst, N);
+}
+
+// Replaces the nearest-point index grid (e.g. one that keeps a sample of the
+// tagged grid points and sets the rest to -1, so that the reference's band
+// drivers evaluate only the sample).
+void refe2g_set_nrst(const int* nrst_grid) { to3(nrst_grid, nrst, g_N); }
+
+// The reference's plain sums (stokes_SL_away, stokes_pressure_away;
+// E2G/stokes.cpp:13-45, 102-126) at arbitrary points, as its box-face drivers
+// call them (E2G/main.cpp:1049-1116, 1218-1299): u (3 per point) and p.
+void refe2g_away_points(int n, const double* xyz, double* u, double* p) {
+  int nq = (int)Surfc.size();
+#pragma omp parallel
+  {
+    vector<double> SL(3, 0.0);
+#pragma omp for schedule(dynamic, 4)
+    for (int i = 0; i < n; i++) {
+      stokes_SL_away(nq, Surfc, f_ex, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], SL);
+      for (int k = 0; k < 3; k++) u[3 * i + k] = SL[k];
+      p[i] = stokes_pressure_away(nq, Surfc, f_ex, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    }
+  }
+}
+
 double refe2g_p_exact(double x, double y, double z) { return p_exact(x, y, z); }
 void refe2g_u_exact(double x, double y, double z, double* u) {
   vector<double> v = SL_exact(x, y, z);

@@ -57,6 +57,26 @@ def make_2s(N=16, P=4, N0=300):
     np.savez_compressed(os.path.join(HERE, "ref2s_N%d_P%d_N0%d.npz" % (N, P, N0)), **out)
 
 
+def make_2s_bench(N=64, P=6, N0=2000, n_sample=4096):
+    """The benchmark's two-surface configuration (h = 1/64, KITC P = 6,
+    N0 = 2000): the reference's GMRES residual history and, at a seeded sample
+    of unknowns, its solution, right-hand side and one operator application
+    (of a seeded density). Only samples are stored: the full vectors are
+    171,054 doubles each."""
+    R = Ref2S(P, N0).setup(N)
+    n = 3 * sum(R.nq)
+    rng = np.random.default_rng(SEED)
+    idx = np.sort(rng.choice(n, n_sample, replace=False)).astype(np.int32)
+    u = np.random.default_rng(SEED + 1).standard_normal(n)
+    out = dict(N=N, P=P, N0=N0, n=n, idx=idx, mv_seed=SEED + 1)
+    out["rhs"] = R.rhs()[idx]
+    out["mv_y"] = R.matvec(u)[idx]
+    x, hist = R.solve()
+    out["sol_x"] = x[idx]
+    out["sol_hist"] = hist
+    np.savez_compressed(os.path.join(HERE, "ref2s_N%d_P%d_N0%d_sampled.npz" % (N, P, N0)), **out)
+
+
 def make_e2g(N=48):
     R = RefE2G().setup(N)
     S = R.surface()
@@ -90,4 +110,5 @@ if __name__ == "__main__":
         sys.exit("reference tree not available; fixtures not regenerated")
     make_2s()
     make_e2g()
+    make_2s_bench()
     print(sorted(os.listdir(HERE)))

@@ -121,3 +121,59 @@ def test_dst_is_involution_up_to_scale(oracle):
     a = np.random.default_rng(3).standard_normal(n ** 3)
     b = oracle.dst1_3d(n, oracle.dst1_3d(n, a))
     assert rel_err(b / (2 * (n + 1)) ** 3, a) < 1e-13
+
+
+def _ref_or_skip(name):
+    import os
+
+    import oracle as oracle_mod
+
+    if not os.path.exists(os.path.join(oracle_mod.REF_DIR, name)):
+        pytest.skip("reference build %s not present" % name)
+    return oracle_mod
+
+
+def test_reference_scene_loader_and_sampled_sums(g2s):
+    """The reference program driven from loaded arrays (ref2s_load) and on a
+    target sample (ref2s_sample_eval) reproduces its own full direct sums and
+    nearest-point densities of the fixture bit for bit."""
+    om = _ref_or_skip("libref2s_P4_N300.so")
+    R = om.Ref2S(4, 300)
+    R.load(g2s, g=[g2s["g0"], g2s["g1"]])
+    for s, t in PAIRS:
+        n = len(g2s["area%d" % t])
+        idx = np.arange(n, dtype=np.int32)[::-1].copy()  # every target, in reverse order
+        sl, _ = R.sample_eval(0, s, t, idx)
+        assert np.array_equal(sl.reshape(-1, 3), g2s["sl_t0_%d%d" % (s, t)].reshape(-1, 3)[idx])
+        dl, g0 = R.sample_eval(1, s, t, idx)
+        assert np.array_equal(dl.reshape(-1, 3), g2s["dl_t0_%d%d" % (s, t)].reshape(-1, 3)[idx])
+        if s != t:
+            assert np.array_equal(g0.reshape(-1, 3), g2s["g0interp%d" % t].reshape(-1, 3)[idx])
+
+
+def test_reference_e2g_loader_and_sampled_sums(ge2g):
+    """The reference extend-to-grid program driven from loaded arrays
+    (refe2g_load) reproduces its own band and face sums of the fixture, on the
+    whole index grid and on a sample of it."""
+    om = _ref_or_skip("librefe2g.so")
+    N = int(ge2g["N"])
+    M = N + 1
+    R = om.RefE2G().load(N, ge2g)
+    p = R.eval_p_band(R.eval_p_faces())
+    assert np.array_equal(p, ge2g["p_band"])
+    nrst = ge2g["nrst"]
+    tagged = np.flatnonzero(nrst >= 0)
+    sample = tagged[::7]
+    keep = np.full_like(nrst, -1)
+    keep[sample] = nrst[sample]
+    R.set_nrst(keep)
+    ps = R.eval_p_band(np.zeros(M ** 3))
+    b = ge2g["b"]
+    out = sample[(b[nrst[sample]] > 0.0) | (np.abs(b[nrst[sample]]) < 1e-12)]
+    assert np.array_equal(ps[out], ge2g["p_band"][out])
+    face = np.array([0, 5 * M + 3, M * M * N + 7 * M + 2, (M * M + M + 1) * N], dtype=np.int64)
+    xyz = np.stack(np.unravel_index(face, (M, M, M)), axis=1).astype(np.float64) * float(ge2g["h"])
+    u, pf = R.away_points(xyz.ravel())
+    assert np.array_equal(pf, ge2g["p_faces"][face])
+    uf = ge2g["u_faces"].reshape(3, -1)[:, face].T.ravel()
+    assert np.array_equal(u, uf)

@@ -55,6 +55,29 @@ def test_noalloc_matches_allocating_entry_point_twice(ctx, ge2g):
     assert rel_err(second, ref2) < TOL
 
 
+def test_noalloc_edge_sizes(ctx):
+    # no sources: one empty chunk, every target gets zeros
+    rng = np.random.default_rng(21)
+    xt = rng.uniform(-2.0, 2.0, 3 * 1000)
+    z = _noalloc(np.zeros(0), np.zeros(0), np.zeros(0), xt)
+    assert np.array_equal(z, np.zeros(len(xt)))
+    # targets near the scratch limit: the source chunks drop from ten to one
+    # (and to two at half the limit), so each target sums its sources in fewer,
+    # longer runs; checked against the allocating entry point
+    nq = 20000
+    xs = rng.uniform(-1.0, 1.0, 3 * nq)
+    area = rng.uniform(0.5, 1.5, nq) * 1e-4
+    f = rng.standard_normal(3 * nq)
+    L = highreg.lib()
+    L.hr_stokeslet_away_noalloc_max_targets.restype = ctypes.c_longlong
+    limit = int(L.hr_stokeslet_away_noalloc_max_targets())
+    for nt in (limit, limit // 2 + 1):
+        xt = rng.uniform(1.5, 3.0, 3 * nt)
+        got = _noalloc(xs, area, f, xt)
+        ref = ctx.e2g_sl_away(xs, area, f, xt)
+        assert rel_err(got, ref) < TOL
+
+
 def test_noalloc_rejects_sizes_beyond_its_scratch():
     L = highreg.lib()
     L.hr_stokeslet_away_noalloc_max_targets.restype = ctypes.c_longlong
