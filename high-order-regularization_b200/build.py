@@ -18,6 +18,7 @@ ROOT = os.path.dirname(HERE)
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhighreg_b200.so")
 REFAPI = os.path.join(HERE, "libhighreg_refapi.so")
+FFTWAPI = os.path.join(HERE, "libhighreg_fftw.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp",
@@ -27,9 +28,11 @@ CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-Wall", "-I", os.path.joi
 
 def _sources():
     cu = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
-    cpp = sorted(f for f in glob.glob(os.path.join(HERE, "host", "*.cpp")) if not f.endswith("hr_ref_api.cpp"))
+    cpp = sorted(f for f in glob.glob(os.path.join(HERE, "host", "*.cpp"))
+                 if not f.endswith(("hr_ref_api.cpp", "hr_fftw_shim.cpp")))
     hdr = sorted(glob.glob(os.path.join(HERE, "csrc", "*.h")) + glob.glob(os.path.join(HERE, "csrc", "*.cuh"))
-                 + glob.glob(os.path.join(HERE, "host", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h")))
+                 + glob.glob(os.path.join(HERE, "host", "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+                 + glob.glob(os.path.join(ROOT, "include", "fftw_shim", "*.h")))
     return cu, cpp, hdr
 
 
@@ -67,6 +70,12 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     if force or not os.path.exists(REFAPI) or os.path.getmtime(REFAPI) < max(os.path.getmtime(src), hdr_t,
                                                                               os.path.getmtime(LIB)):
         logs.append(_run(["g++"] + CXXFLAGS + ["-shared", src, "-o", REFAPI, "-L", HERE, "-lhighreg_b200",
+                          "-Wl,-rpath,$ORIGIN"], verbose))
+    # the FFTW-API layer (fftw_plan_r2r_3d / fftw_execute ... over hr_dst1_*)
+    src = os.path.join(HERE, "host", "hr_fftw_shim.cpp")
+    if force or not os.path.exists(FFTWAPI) or os.path.getmtime(FFTWAPI) < max(os.path.getmtime(src), hdr_t,
+                                                                                os.path.getmtime(LIB)):
+        logs.append(_run(["g++"] + CXXFLAGS + ["-shared", src, "-o", FFTWAPI, "-L", HERE, "-lhighreg_b200",
                           "-Wl,-rpath,$ORIGIN"], verbose))
     if ptxas_info:
         print("\n".join(l for l in logs if l))

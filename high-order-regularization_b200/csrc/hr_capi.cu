@@ -20,6 +20,10 @@ using namespace hr;
 namespace hr {
 // implemented in hr_poisson.cu
 void dst_poisson3d_dev(Ctx& C, int n, double* f_dev);
+struct Dst1Plan;
+Dst1Plan* dst1_plan_create(Ctx& C, int n);
+void dst1_plan_destroy(Dst1Plan* D);
+void dst1_execute(Ctx& C, Dst1Plan* D, const double* in_host, double* out_host);
 
 }  // namespace hr
 
@@ -398,6 +402,57 @@ extern "C" int hr_dst_poisson3d(hr_ctx* ctx, int n, double* f) {
     HR_CHECK_CUDA(cudaMemcpyAsync(f, d.p, m * sizeof(double), cudaMemcpyDeviceToHost, st));
     HR_CHECK_CUDA(cudaStreamSynchronize(st));
   });
+}
+
+struct hr_dst1_plan {
+  hr_ctx* ctx = nullptr;
+  hr::Dst1Plan* d = nullptr;
+  ~hr_dst1_plan() {
+    if (d) hr::dst1_plan_destroy(d);
+  }
+};
+
+extern "C" int hr_dst1_plan_create(hr_ctx* ctx, int n, hr_dst1_plan** out) {
+  if (!ctx || !out) return HR_ERR_ARG;
+  *out = nullptr;
+  return guard(ctx, [&] {
+    HR_REQUIRE(n >= 1 && (n + 1) % 2 == 0, "3D DST-I length n must have n + 1 even");
+    HR_CHECK_CUDA(cudaSetDevice(ctx->c.device));
+    std::unique_ptr<hr_dst1_plan> p(new hr_dst1_plan);
+    p->ctx = ctx;
+    p->d = dst1_plan_create(ctx->c, n);
+    *out = p.release();
+  });
+}
+
+extern "C" int hr_dst1_execute(hr_dst1_plan* p, const double* in, double* out) {
+  if (!p || !in || !out) return HR_ERR_ARG;
+  return guard(p->ctx, [&] {
+    HR_CHECK_CUDA(cudaSetDevice(p->ctx->c.device));
+    dst1_execute(p->ctx->c, p->d, in, out);
+  });
+}
+
+extern "C" int hr_host_alloc(size_t bytes, void** out) {
+  if (!out) return HR_ERR_ARG;
+  *out = nullptr;
+  if (cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    *out = nullptr;
+    return HR_ERR_CUDA;
+  }
+  return HR_OK;
+}
+
+extern "C" void hr_host_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+
+extern "C" void hr_dst1_plan_destroy(hr_dst1_plan* p) {
+  if (!p) return;
+  cudaSetDevice(p->ctx->c.device);
+  cudaStreamSynchronize(p->ctx->c.stream);
+  delete p;
 }
 
 extern "C" int hr_e2g_solve_poisson(hr_ctx* ctx, int N, double L, const uint8_t* band2,

@@ -538,6 +538,35 @@ void dst_poisson3d_dev(Ctx& C, int n, double* f_dev) {
   HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
 }
 
+// A plain 3D DST-I (FFTW's RODFT00 on all three axes, unnormalised) of an
+// n^3 row-major array: three passes in mode 0, alternating between the data
+// and the plan's scratch grid, so the result lands in the scratch grid and the
+// layout is restored. Tables and buffers are kept for repeated executions
+// (the FFTW-API layer keeps one per fftw_plan).
+struct Dst1Plan {
+  DstPlan P;
+  DBuf<double> a;
+};
+
+Dst1Plan* dst1_plan_create(Ctx& C, int n) {
+  std::unique_ptr<Dst1Plan> D(new Dst1Plan);
+  D->P.make(C, n);
+  D->a.alloc((size_t)n * n * n);
+  return D.release();
+}
+
+void dst1_plan_destroy(Dst1Plan* D) { delete D; }
+
+void dst1_execute(Ctx& C, Dst1Plan* D, const double* in_host, double* out_host) {
+  const size_t m = (size_t)D->P.n * D->P.n * D->P.n;
+  HR_CHECK_CUDA(cudaMemcpyAsync(D->a.p, in_host, m * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+  D->P.pass(C, D->a.p, D->P.tmp.p, 0, 0.0, nullptr, nullptr);
+  D->P.pass(C, D->P.tmp.p, D->a.p, 0, 0.0, nullptr, nullptr);
+  D->P.pass(C, D->a.p, D->P.tmp.p, 0, 0.0, nullptr, nullptr);
+  HR_CHECK_CUDA(cudaMemcpyAsync(out_host, D->P.tmp.p, m * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+  HR_CHECK_CUDA(cudaStreamSynchronize(C.stream));
+}
+
 // The twiddle tables and grid work buffers of one grid size, kept across
 // solves (a pipeline runs four solves per evaluation).
 struct PoissonWork {

@@ -126,6 +126,21 @@ int hr_e2g_pressure_7ord(hr_ctx* ctx, double delta, const hr_surface* S, const d
  * n^3 host array: DST-I, divide by the eigenvalues of the 4th-order compact
  * Laplacian, DST-I, scale 1/(2(n+1))^3. */
 int hr_dst_poisson3d(hr_ctx* ctx, int n, double* f);
+/* A plain 3D DST-I, FFTW's RODFT00 on all three axes, unnormalised
+ * (Y = 2 sum X_j sin(pi (j+1)(k+1)/(n+1)) per axis), of a row-major n^3 host
+ * array: what fftw_plan_r2r_3d(n, n, n, in, out, FFTW_RODFT00 x3, ...) +
+ * fftw_execute compute in E2G/main.cpp:1429-1471. The plan keeps its device
+ * tables and buffers; each execute copies in, runs three fused DST passes and
+ * copies out (in == out allowed). n + 1 must be even (the grids' N = n + 1). */
+typedef struct hr_dst1_plan hr_dst1_plan;
+int hr_dst1_plan_create(hr_ctx* ctx, int n, hr_dst1_plan** out);
+int hr_dst1_execute(hr_dst1_plan* p, const double* in, double* out);
+void hr_dst1_plan_destroy(hr_dst1_plan* p);
+/* Page-locked host memory (cudaHostAlloc / cudaFreeHost), for callers that
+ * stage arrays to the library without linking the CUDA runtime themselves
+ * (the FFTW-API layer's fftw_malloc / fftw_free). */
+int hr_host_alloc(size_t bytes, void** out);
+void hr_host_free(void* p);
 
 /* solve_Poisson: E2G/main.cpp:969-1044. Grids are row-major (N+1)^3.
  * band2: 1 at BAND2 points; outside: 1 at exterior points outside BAND2

@@ -157,6 +157,34 @@ def build_relinked_reference(force: bool = False, root: str | None = None):
     return out
 
 
+def build_relinked_e2g(force: bool = False, root: str | None = None):
+    """The reference's unmodified extend-to-grid driver (main.cpp, stokes.cpp,
+    surface.cpp, utilities.cpp: its own CPU boundary sums) compiled against
+    the product's FFTW-API header and linked against libhighreg_fftw.so
+    instead of FFTW, so that its Poisson solves (fftw_DST_Poisson3d_FD) run
+    their transforms on the B200: the drop-in test of the Poisson boundary.
+    Needs the reference tree and the built product libraries; returns the
+    binary path or None."""
+    root = reference_root(root)
+    if root is None:
+        return None
+    e2g = os.path.join(root, "highreg_stokes_extend_to_grid")
+    repo = os.path.dirname(HERE)
+    pkg = os.path.join(repo, "high-order-regularization_b200")
+    lib = os.path.join(pkg, "libhighreg_fftw.so")
+    if not os.path.isdir(e2g) or not os.path.exists(lib):
+        return None
+    os.makedirs(REF_OUT, exist_ok=True)
+    out = os.path.join(REF_OUT, "refe2g_main_relinked")
+    srcs = [os.path.join(e2g, f) for f in ("main.cpp", "stokes.cpp", "surface.cpp", "utilities.cpp")]
+    if force or not _newer(out, srcs + [lib]):
+        _run(["g++", "-std=c++14", "-O2", "-fopenmp", "-w", "-I", e2g,
+              "-I", os.path.join(repo, "include", "fftw_shim")] + srcs
+             + ["-o", out, "-L", pkg, "-lhighreg_fftw", "-lhighreg_b200", "-Wl,-rpath," + pkg,
+                "-Wl,-rpath,$ORIGIN/../../high-order-regularization_b200"])
+    return out
+
+
 def build_all(force: bool = False) -> None:
     build_checker(force)
     build_reference(force)

@@ -87,3 +87,26 @@ def test_geometry_rejects_bad_arguments():
     out = ctypes.c_void_p()
     assert L.hr_geom2s_generate(ctypes.byref(p), 1, ctypes.byref(out)) == highreg.HR_ERR_ARG
     assert L.hr_geom2s_generate(None, 16, ctypes.byref(out)) == highreg.HR_ERR_ARG
+
+
+def test_fftw_layer_exports_its_header():
+    """libhighreg_fftw.so exports every function include/fftw_shim/fftw3.h
+    declares, with C linkage (FFTW's names, so a driver links it in place of
+    -lfftw3); loading it needs no GPU."""
+    import ctypes
+
+    path = os.path.join(ROOT, "high-order-regularization_b200", "libhighreg_fftw.so")
+    L = ctypes.CDLL(path)
+    txt = open(os.path.join(ROOT, "include", "fftw_shim", "fftw3.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    names = sorted(set(re.findall(r"\b(fftw_[a-z0-9_]+)\s*\(", txt)))
+    assert names == ["fftw_cleanup", "fftw_destroy_plan", "fftw_execute", "fftw_free", "fftw_malloc",
+                     "fftw_plan_r2r_3d"]
+    for n in names:
+        assert hasattr(L, n), n
+    # unsupported plans are refused before any device work
+    L.fftw_plan_r2r_3d.restype = ctypes.c_void_p
+    buf = (ctypes.c_double * 64)()
+    assert L.fftw_plan_r2r_3d(4, 4, 4, buf, buf, 7, 7, 7, 64) is None      # n + 1 odd
+    assert L.fftw_plan_r2r_3d(3, 3, 5, buf, buf, 7, 7, 7, 64) is None      # not a cube
+    assert L.fftw_plan_r2r_3d(3, 3, 3, buf, buf, 3, 7, 7, 64) is None      # not RODFT00

@@ -40,3 +40,42 @@ def test_reference_driver_on_gpu(tmp_path, oracle):
     v1 = np.loadtxt(os.path.join(tmp_path, "vel1_N32_highreg_57_k4")).ravel()
     v2 = np.loadtxt(os.path.join(tmp_path, "vel2_N32_highreg_57_k4")).ravel()
     assert rel_err(np.concatenate([v1, v2]), x) < 1e-9
+
+
+E2G_EXE = os.path.join(ROOT, "oracle", "_ref", "refe2g_main_relinked")
+
+
+def _error_lines(text):
+    """(line text without numbers, numbers) of every printed error line."""
+    num = r"[-+]?\d+\.?\d*(?:[eE][-+]?\d+)?"
+    out = []
+    for line in text.splitlines():
+        if "err" in line and "time" not in line.lower():
+            out.append((re.sub(num, "#", line).strip(), [float(v) for v in re.findall(num, line)]))
+    return out
+
+
+@pytest.mark.skipif(not os.path.exists(E2G_EXE), reason="relinked reference extend-to-grid driver not built")
+def test_reference_e2g_driver_with_gpu_poisson(tmp_path):
+    """The reference's unmodified extend-to-grid driver (N = 96, its own CPU
+    boundary sums) relinked against the FFTW-API layer, so that every DST-I
+    of its four Poisson solves runs on the B200: its printed error tables
+    equal those of the same driver on the CPU DST-I stand-in (the reference
+    built with oracle/fftw_standin), among them the reference's table
+    (u in the band: max 4.2629e-04; u on the grid: max 4.34278e-04; p on the
+    grid: max 2.9393e-03). Lines that print times are not compared."""
+    import oracle as om
+
+    env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()))
+    r = subprocess.run([E2G_EXE], cwd=tmp_path, capture_output=True, text=True, timeout=900, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "B200 layer" not in r.stderr, r.stderr[-2000:]
+    got = _error_lines(r.stdout)
+    R = om.RefE2G().setup(96)
+    ref = _error_lines(R.run())
+    assert len(got) == len(ref) and len(got) >= 6
+    for (lg, vg), (lr, vr) in zip(got, ref):
+        assert lg == lr
+        assert np.allclose(vg, vr, rtol=2e-5, atol=0), (lg, vg, vr)
+    text = r.stdout
+    assert "max err (u) = 0.000434278" in text and "max err (p) = 0.0029393" in text, text[-3000:]
