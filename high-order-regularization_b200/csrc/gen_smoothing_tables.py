@@ -106,6 +106,49 @@ def build(f):
     return out, worst
 
 
+# FP64 tables centred on a uniform grid in s, for an index formed by one
+# fused multiply-add: piece i (i = 0 .. NI) is centred at c_i = i * 64 / NI
+# and covers s in [c_i - w/2, c_i + w/2] (w = 64 / NI), so the piece of s is
+# round-to-nearest(s * NI / 64) and t = s - c_i needs no stored centre. Each
+# piece is DEG + 1 monomial coefficients in t, the interpolant at DEG + 1
+# Chebyshev nodes of the piece widened by 0.2 % of w at each end (80 digits).
+GRID_TABLES = {"G1": (64, 13), "G2": (64, 13), "G3": (256, 9)}
+
+
+def piece_grid(f, i, ni, deg):
+    w = mp.mpf(64) / ni
+    c = i * w
+    slo = max(mp.mpf(0), c - w / 2 - w * mp.mpf("0.002"))
+    shi = c + w / 2 + w * mp.mpf("0.002")
+    half, mid = (shi - slo) / 2, (shi + slo) / 2
+    n = deg + 1
+    ts = [mid + half * mp.cos(mp.pi * (k + mp.mpf(1) / 2) / n) - c for k in range(n)]
+    V = mp.matrix(n, n)
+    for r, t in enumerate(ts):
+        for j in range(n):
+            V[r, j] = t ** j
+    coef = mp.lu_solve(V, mp.matrix([f(t + c) for t in ts]))
+    return [coef[j] for j in range(n)], c
+
+
+def build_grid(f, ni, deg):
+    """Rounded coefficients of pieces 0 .. ni and the worst relative error of
+    their exact evaluation over 21 points per piece within [0, 64]."""
+    out, worst = [], mp.mpf(0)
+    w = mp.mpf(64) / ni
+    for i in range(ni + 1):
+        coef, c = piece_grid(f, i, ni, deg)
+        cd = [float(a) for a in coef]
+        for k in range(21):
+            sv = mp.mpf(float(c - w / 2 + w * k / 20))
+            if sv < 0 or sv > 64:
+                continue
+            ex = f(sv)
+            worst = max(worst, abs(horner([mp.mpf(a) for a in cd], sv - c) - ex) / abs(ex))
+        out.append(cd)
+    return out, worst
+
+
 # FP32 tables for the mixed-precision path: NI32 pieces uniform in s (index
 # floor(s * NI32 / 64), no square root), degree DEG32, each piece stored as
 # 8 floats (centre, coefficients of t^0 .. t^5, 0) = two float4.
@@ -166,6 +209,18 @@ def main():
         lines.append("HR_SMOOTH_STORAGE double kSmooth%s[%d * %d] = {" % (name, NI, DEG + 2))
         for c, cd in tab:
             lines.append("    " + ", ".join(repr(v) for v in [c] + cd) + ",")
+        lines.append("};")
+    for name, f in (("G1", G1), ("G2", G2), ("G3", G3)):
+        ni, deg = GRID_TABLES[name]
+        tab, worst = build_grid(f, ni, deg)
+        lines.append("// %s on the s grid: pieces 0 .. %d centred at i * %g, degree %d; max relative error %.2e"
+                     % (name, ni, 64.0 / ni, deg, float(worst)))
+        print(name, "grid max rel err", float(worst))
+        lines.append("#define HR_SMOOTHS_%s_PIECES %d" % (name, ni))
+        lines.append("#define HR_SMOOTHS_%s_DEG %d" % (name, deg))
+        lines.append("HR_SMOOTH_STORAGE double kSmoothS%s[%d * %d] = {" % (name, ni + 1, deg + 1))
+        for cd in tab:
+            lines.append("    " + ", ".join(repr(v) for v in cd) + ",")
         lines.append("};")
     lines.append("// FP32 tables: %d pieces uniform in s (width %g), degree %d; per piece 8 floats:"
                  % (NI32, 64.0 / NI32, DEG32))

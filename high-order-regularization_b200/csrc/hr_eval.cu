@@ -38,16 +38,54 @@ namespace {
 
 // On-surface smoothing factors without erf / exp / rsqrt: for r <= 8 delta,
 // s1 = G1(s) / delta, s2 = G2(s) / delta^3, s3 = G3(s) / delta^5 with
-// s = r^2 / delta^2, each G a piecewise polynomial (64 pieces uniform in
-// r/delta, degree 11 in s - centre) fitted in 80-digit arithmetic to the
-// reference's formulas (2S/utilities.cpp:211-254, :292-323) with ~1e-16
-// relative error; G(0) is the reference's r -> 0 value. The table of a kernel
-// family is staged in shared memory once per CTA.
-constexpr int kSmoothN = HR_SMOOTH_PIECES * (HR_SMOOTH_DEG + 2);  // doubles per table (global)
-// shared-memory copy: each piece padded to an even length, read as double2
-constexpr int kSmoothW = HR_SMOOTH_DEG + 3;
-constexpr int kSmoothNs = HR_SMOOTH_PIECES * kSmoothW;
-static_assert(kSmoothW % 2 == 0, "a padded piece must be whole double2s");
+// s = r^2 / delta^2, each G a piecewise polynomial fitted in 80-digit
+// arithmetic to the reference's formulas (2S/utilities.cpp:211-254,
+// :292-323) with ~1e-16 relative error; G(0) is the reference's r -> 0 value.
+// Piece i of a table is centred at s = i w (w = 64 / NI; G1, G2: NI = 64,
+// degree 13; G3: NI = 256, degree 9), so the piece of s is
+// round-to-nearest(s / w), formed with one fused multiply-add (adding
+// 1.5 * 2^52 leaves the rounded integer in the low word), and t = s - i w
+// follows from the same sum without a stored centre. The tables of a kernel
+// family are staged in shared memory once per CTA, with the powers of
+// 1/delta folded into the coefficients.
+template <int NI, int DEG>
+struct SmoothTab {
+  static constexpr int kPieces = NI;
+  static constexpr int kCoef = DEG + 1;  // coefficients per piece (even: whole double2s)
+  static constexpr int kLen = (NI + 1) * kCoef;
+  static_assert(kCoef % 2 == 0, "a piece must be whole double2s");
+};
+using TabG1 = SmoothTab<HR_SMOOTHS_G1_PIECES, HR_SMOOTHS_G1_DEG>;
+using TabG2 = SmoothTab<HR_SMOOTHS_G2_PIECES, HR_SMOOTHS_G2_DEG>;
+using TabG3 = SmoothTab<HR_SMOOTHS_G3_PIECES, HR_SMOOTHS_G3_DEG>;
+static_assert(TabG1::kPieces == TabG2::kPieces && TabG1::kLen == TabG2::kLen, "G1 and G2 share their pieces");
+static_assert((TabG1::kLen * 8) % 16 == 0, "the G2 table must start on a double2");
+
+constexpr double kRoundMagic = 6755399441055744.0;  // 1.5 * 2^52
+
+// Piece index and offset of s >= 0 (s <= 64) on the grid of NI pieces.
+template <int NI>
+__device__ __forceinline__ int smooth_piece(double s, double& t) {
+  const double f = fma(s, NI / 64.0, kRoundMagic);  // kRoundMagic + round(s NI / 64), exact
+  t = fma(kRoundMagic - f, 64.0 / NI, s);           // s - i w
+  return min(__double2loint(f), NI);
+}
+
+template <class TAB>
+__device__ __forceinline__ double smooth_horner(const double* __restrict__ tab, int i, double t) {
+  const double2* p2 = reinterpret_cast<const double2*>(tab + i * TAB::kCoef);
+  double e[TAB::kCoef];
+#pragma unroll
+  for (int k = 0; k < TAB::kCoef / 2; k++) {
+    const double2 v = p2[k];
+    e[2 * k] = v.x;
+    e[2 * k + 1] = v.y;
+  }
+  double v = e[TAB::kCoef - 1];
+#pragma unroll
+  for (int k = TAB::kCoef - 2; k >= 0; k--) v = fma(v, t, e[k]);
+  return v;
+}
 
 constexpr int kSmooth32N = HR_SMOOTH32_PIECES * 8;  // floats per FP32 table
 
@@ -62,25 +100,6 @@ __device__ __forceinline__ float smooth_eval_f(const float4* __restrict__ tab, f
   const float4 a = tab[2 * i], b = tab[2 * i + 1];
   const float t = s - a.x;
   return fmaf(fmaf(fmaf(fmaf(fmaf(b.z, t, b.y), t, b.x), t, a.w), t, a.z), t, a.y);
-}
-
-// FP64 piece in shared memory: (centre, c0) (c1, c2) ... (c11, 0) as double2.
-__device__ __forceinline__ double smooth_eval(const double* __restrict__ tab, double s) {
-  int i = (int)(sqrtf((float)s) * (HR_SMOOTH_PIECES / 8.0f));
-  i = min(max(i, 0), HR_SMOOTH_PIECES - 1);
-  const double2* p2 = reinterpret_cast<const double2*>(tab + i * kSmoothW);
-  double e[kSmoothW];
-#pragma unroll
-  for (int k = 0; k < kSmoothW / 2; k++) {
-    const double2 v = p2[k];
-    e[2 * k] = v.x;
-    e[2 * k + 1] = v.y;
-  }
-  const double t = s - e[0];
-  double v = e[HR_SMOOTH_DEG + 1];
-#pragma unroll
-  for (int k = HR_SMOOTH_DEG; k >= 1; k--) v = fma(v, t, e[k]);
-  return v;
 }
 
 constexpr int kWarps = kTB / 32;     // warps per CTA, each with its own tiles
@@ -210,9 +229,10 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       H1 = ri;
       H2 = ri * ri * ri;
     } else {
-      const double sq = r2 * g.inv_d2;
-      H1 = smooth_eval(stab, sq);
-      H2 = smooth_eval(stab + kSmoothNs, sq);
+      double t;
+      const int i = smooth_piece<TabG1::kPieces>(r2 * g.inv_d2, t);
+      H1 = smooth_horner<TabG1>(stab, i, t);
+      H2 = smooth_horner<TabG2>(stab + TabG1::kLen, i, t);
     }
     reg = r2 <= g.d64 && r2 >= g.r0sq;  // the reference's branch (work counters)
     H2 *= fdd;
@@ -254,7 +274,9 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
       const double ri = rsqrt(r2), ri2 = ri * ri;
       H3 = ri2 * ri2 * ri;
     } else {
-      H3 = smooth_eval(stab, r2 * g.inv_d2);
+      double t;
+      const int i = smooth_piece<TabG3::kPieces>(r2 * g.inv_d2, t);
+      H3 = smooth_horner<TabG3>(stab, i, t);
     }
     reg = r2 <= g.d64 && r2 >= g.r0sq;  // the reference's branch (work counters)
     const double kernel = ndd * gdd * H3;
@@ -1093,25 +1115,23 @@ __global__ void __launch_bounds__(kTB, ON ? (FAM == F_E2G ? 6 : 5) : 4)
   __shared__ float chebf[kWarps * 3 * kMaxP1];
   __shared__ EvalTask sT;
   // smoothing tables: G1, G2 for the Stokeslet family, G3 for the stresslet family
-  __shared__ __align__(16) double stab[FAM == F_SL ? 2 * kSmoothNs : (FAM == F_DL ? kSmoothNs : 2)];
+  __shared__ __align__(16) double stab[(FAM == F_SL && ON) ? TabG1::kLen + TabG2::kLen
+                                                            : ((FAM == F_DL && ON) ? TabG3::kLen : 2)];
   __shared__ float4 stab32[MIXED ? (FAM == F_SL ? 2 * kSmooth32N / 4 : (FAM == F_DL ? kSmooth32N / 4 : 1)) : 1];
   const BlockRef it = items[blockIdx.x];
   if (threadIdx.x == 0) sT = tasks[it.task];
-  // The tables carry the powers of 1/delta of the factors they give: the
-  // coefficients (not the piece centres) are scaled by 1/delta, 1/delta^3
-  // (G1, G2) or 1/delta^5 (G3) while they are staged.
+  // The tables carry the powers of 1/delta of the factors they give: every
+  // coefficient is scaled by 1/delta, 1/delta^3 (G1, G2) or 1/delta^5 (G3)
+  // while they are staged.
   if ((FAM == F_SL || FAM == F_DL) && ON) {
     const Reg gs = make_reg(tasks[it.task].DEL);
-    for (int i = threadIdx.x; i < kSmoothNs; i += blockDim.x) {
-      const int piece = i / kSmoothW, k = i - piece * kSmoothW;
-      const int src = piece * (HR_SMOOTH_DEG + 2) + k;
-      const bool pad = k == kSmoothW - 1;
-      if (FAM == F_SL) {
-        stab[i] = pad ? 0.0 : kSmoothG1[src] * (k == 0 ? 1.0 : gs.inv_d);
-        stab[kSmoothNs + i] = pad ? 0.0 : kSmoothG2[src] * (k == 0 ? 1.0 : gs.inv_d3);
-      } else {
-        stab[i] = pad ? 0.0 : kSmoothG3[src] * (k == 0 ? 1.0 : gs.inv_d5);
+    if (FAM == F_SL) {
+      for (int i = threadIdx.x; i < TabG1::kLen; i += blockDim.x) {
+        stab[i] = kSmoothSG1[i] * gs.inv_d;
+        stab[TabG1::kLen + i] = kSmoothSG2[i] * gs.inv_d3;
       }
+    } else {
+      for (int i = threadIdx.x; i < TabG3::kLen; i += blockDim.x) stab[i] = kSmoothSG3[i] * gs.inv_d5;
     }
     if (MIXED) {
       float* t32 = reinterpret_cast<float*>(stab32);

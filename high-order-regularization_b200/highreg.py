@@ -366,6 +366,10 @@ class Geometry2S:
             d["nrst%d" % s] = np.ctypeslib.as_array(T.nrst, (n,)).copy()
             d["i123%d" % s] = np.ctypeslib.as_array(T.i123, (3 * n,)).copy()
         self.scene = d
+        ph = (ctypes.c_double * 4)()
+        L.hr_geom2s_phase_seconds(p, ph)
+        # wall seconds of the set-up phases: quadrature, forces, nearest data of sets 0 and 1
+        self.phase_seconds = {"quadrature": ph[0], "forces": ph[1], "nearest0": ph[2], "nearest1": ph[3]}
         L.hr_geom2s_destroy(p)
         self.p = None
 

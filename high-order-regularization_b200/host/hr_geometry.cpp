@@ -15,6 +15,8 @@
 #include <memory>
 #include <vector>
 
+#include <omp.h>
+
 #include "../../include/highreg_b200.h"
 
 namespace {
@@ -399,88 +401,109 @@ void surface_force(const Spheroid& S, const double axes[3], const double* x0, co
 }
 
 // find_Nearest_grid (2S/surface.cpp:370-390): nearest quadrature point of a
-// plane family, first index on ties, none beyond distance^2 = 100. A
-// best-first search over occupied cells of a uniform grid returns the same
-// index as the reference's linear scan.
-struct CellIndex {
-  double lo[3], cs;
-  int G;
-  std::vector<int> cell_of_pt;
-  std::vector<std::vector<int>> cells[3];  // per plane family: occupied cell ids
-  std::vector<std::vector<int>> members[3];
-  std::vector<double> box[3];              // per occupied cell: 6 bounds
-  void build(const std::vector<QPoint>& P) {
-    double hi[3] = {-1e300, -1e300, -1e300};
-    for (int k = 0; k < 3; k++) lo[k] = 1e300;
-    for (auto& q : P)
+// plane family, first index on ties, none beyond distance^2 = 100. A k-d
+// tree over each family's points (median splits on the widest axis, leaves of
+// at most kLeaf points, tight bounding boxes) is searched nearer child first;
+// a subtree is skipped only when the squared distance from the point to its
+// box exceeds the best squared distance found so far by more than a 1e-12
+// relative margin (for rounding), so every point at the best distance is met
+// and the lowest index among equals wins: the same index as the reference's
+// linear scan.
+struct PointTree {
+  static constexpr int kLeaf = 16;
+  struct Node {
+    double lo[3], hi[3];
+    int child[2];  // -1 for a leaf
+    int begin, end;
+  };
+  std::vector<Node> nodes[3];  // per plane family; node 0 is the root
+  std::vector<int> ids[3];     // point indices in leaf order
+  std::vector<double> pts[3];  // their coordinates, packed in the same order
+
+  int make(int f, const std::vector<QPoint>& P, int b, int e) {
+    Node nd;
+    for (int k = 0; k < 3; k++) {
+      nd.lo[k] = 1e300;
+      nd.hi[k] = -1e300;
+    }
+    for (int i = b; i < e; i++)
       for (int k = 0; k < 3; k++) {
-        lo[k] = std::min(lo[k], q.x[k]);
-        hi[k] = std::max(hi[k], q.x[k]);
+        nd.lo[k] = std::min(nd.lo[k], P[ids[f][i]].x[k]);
+        nd.hi[k] = std::max(nd.hi[k], P[ids[f][i]].x[k]);
       }
-    double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
-    G = 24;
-    cs = ext / G * (1.0 + 1e-9) + 1e-12;
+    nd.child[0] = nd.child[1] = -1;
+    nd.begin = b;
+    nd.end = e;
+    const int me = (int)nodes[f].size();
+    nodes[f].push_back(nd);
+    if (e - b > kLeaf) {
+      int ax = 0;
+      for (int k = 1; k < 3; k++)
+        if (nd.hi[k] - nd.lo[k] > nd.hi[ax] - nd.lo[ax]) ax = k;
+      const int mid = (b + e) / 2;
+      std::nth_element(ids[f].begin() + b, ids[f].begin() + mid, ids[f].begin() + e,
+                       [&](int u, int v) { return P[u].x[ax] < P[v].x[ax]; });
+      const int l = make(f, P, b, mid);
+      const int r = make(f, P, mid, e);
+      nodes[f][me].child[0] = l;
+      nodes[f][me].child[1] = r;
+    }
+    return me;
+  }
+
+  void build(const std::vector<QPoint>& P) {
     for (int f = 0; f < 3; f++) {
-      std::vector<int> slot((size_t)G * G * G, -1);
-      for (size_t j = 0; j < P.size(); j++) {
-        if (P[j].plane != f) continue;
-        int c[3];
-        for (int k = 0; k < 3; k++) c[k] = std::min(G - 1, std::max(0, (int)((P[j].x[k] - lo[k]) / cs)));
-        int id = (c[0] * G + c[1]) * G + c[2];
-        if (slot[id] < 0) {
-          slot[id] = (int)members[f].size();
-          members[f].emplace_back();
-          box[f].insert(box[f].end(), {1e300, -1e300, 1e300, -1e300, 1e300, -1e300});
-        }
-        int s = slot[id];
-        members[f][s].push_back((int)j);
-        double* b = &box[f][6 * s];
-        for (int k = 0; k < 3; k++) {
-          b[2 * k] = std::min(b[2 * k], P[j].x[k]);
-          b[2 * k + 1] = std::max(b[2 * k + 1], P[j].x[k]);
-        }
-      }
+      ids[f].clear();
+      nodes[f].clear();
+      for (size_t j = 0; j < P.size(); j++)
+        if (P[j].plane == f) ids[f].push_back((int)j);
+      if (!ids[f].empty()) make(f, P, 0, (int)ids[f].size());
+      pts[f].resize(3 * ids[f].size());
+      for (size_t i = 0; i < ids[f].size(); i++)
+        for (int k = 0; k < 3; k++) pts[f][3 * i + k] = P[ids[f][i]].x[k];
     }
   }
-  // The point of family f nearest to pt (squared distance below 100), the
-  // lowest index among equals: the reference's linear scan
-  // (2S/surface.cpp:370-390). The answer does not depend on the order in which
-  // points are met, so the cell closest to pt is scanned first, then every
-  // cell whose box can still hold a point as close (box distances carry a
-  // 1e-12 relative margin for rounding).
-  int nearest(const std::vector<QPoint>& P, const double* pt, int f, std::vector<double>& d2c) const {
-    const int nc = (int)members[f].size();
-    d2c.resize(nc);
-    int c0 = -1;
-    for (int c = 0; c < nc; c++) {
-      const double* b = &box[f][6 * c];
-      double d2 = 0;
-      for (int k = 0; k < 3; k++) {
-        double d = 0;
-        if (pt[k] < b[2 * k]) d = b[2 * k] - pt[k];
-        else if (pt[k] > b[2 * k + 1]) d = pt[k] - b[2 * k + 1];
-        d2 += d * d;
-      }
-      d2c[c] = d2;
-      if (c0 < 0 || d2 < d2c[c0]) c0 = c;
+
+  static double box_d2(const Node& nd, const double* pt) {
+    double d2 = 0;
+    for (int k = 0; k < 3; k++) {
+      double d = 0;
+      if (pt[k] < nd.lo[k]) d = nd.lo[k] - pt[k];
+      else if (pt[k] > nd.hi[k]) d = pt[k] - nd.hi[k];
+      d2 += d * d;
     }
+    return d2;
+  }
+
+  int nearest(const double* pt, int f) const {
+    if (nodes[f].empty()) return -1;
     int i0 = -1;
     double best = 100.0;
-    auto scan = [&](int c) {
-      for (int j : members[f][c]) {
-        const double* x = P[j].x;
-        double dist = (pt[0] - x[0]) * (pt[0] - x[0]) + (pt[1] - x[1]) * (pt[1] - x[1]) +
-                      (pt[2] - x[2]) * (pt[2] - x[2]);
-        if (dist < best || (dist == best && i0 >= 0 && j < i0)) {
-          best = dist;
-          i0 = j;
+    int stack[128];
+    int top = 0;
+    stack[top++] = 0;
+    while (top > 0) {
+      const Node& nd = nodes[f][stack[--top]];
+      if (box_d2(nd, pt) > best * (1.0 + 1e-12) + 1e-300) continue;
+      if (nd.child[0] < 0) {
+        for (int i = nd.begin; i < nd.end; i++) {
+          const double* x = &pts[f][3 * i];
+          const int j = ids[f][i];
+          double dist = (pt[0] - x[0]) * (pt[0] - x[0]) + (pt[1] - x[1]) * (pt[1] - x[1]) +
+                        (pt[2] - x[2]) * (pt[2] - x[2]);
+          if (dist < best || (dist == best && i0 >= 0 && j < i0)) {
+            best = dist;
+            i0 = j;
+          }
         }
+        continue;
       }
-    };
-    if (c0 < 0) return -1;
-    scan(c0);
-    for (int c = 0; c < nc; c++)
-      if (c != c0 && d2c[c] <= best * (1.0 + 1e-12) + 1e-300) scan(c);
+      // push the farther child first so the nearer one is searched first
+      const int a = nd.child[0], b = nd.child[1];
+      const bool a_near = box_d2(nodes[f][a], pt) <= box_d2(nodes[f][b], pt);
+      stack[top++] = a_near ? b : a;
+      stack[top++] = a_near ? a : b;
+    }
     return i0;
   }
 };
@@ -495,6 +518,9 @@ struct hr_geom2s {
   std::vector<int> plane[2];
   std::vector<double> b[2], x0[2], n0[2], f0[2];
   std::vector<int> nrst[2], i123[2];
+  // wall seconds of the set-up phases: quadrature (both surfaces), forces,
+  // nearest data of target sets 0 and 1
+  double phase_s[4] = {0, 0, 0, 0};
 };
 
 extern "C" int hr_geom2s_default_params(hr_geom2s_params* p) {
@@ -552,14 +578,18 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
   }
   std::vector<QPoint> P[2];
   const double zero[3] = {0, 0, 0};
+  double t0 = omp_get_wtime();
+  for (int s = 0; s < 2; s++) P[s] = generate_surface(gen[s], N, G->h, zero, prm->center[s]);
+  double t1 = omp_get_wtime();
+  G->phase_s[0] = t1 - t0;
   for (int s = 0; s < 2; s++) {
-    P[s] = generate_surface(gen[s], N, G->h, zero, prm->center[s]);
     const int n = (int)P[s].size();
     G->xyz[s].resize(3 * n);
     G->nrm[s].resize(3 * n);
     G->area[s].resize(n);
     G->plane[s].resize(n);
     G->f[s].resize(3 * n);
+#pragma omp parallel for schedule(static, 256)
     for (int i = 0; i < n; i++) {
       for (int k = 0; k < 3; k++) {
         G->xyz[s][3 * i + k] = P[s][i].x[k];
@@ -571,11 +601,13 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
       surface_force(cen[s], prm->axes, P[s][i].x, P[s][i].n, &G->f[s][3 * i], prm->tension_body != 0);
     }
   }
+  t0 = omp_get_wtime();
+  G->phase_s[1] = t0 - t1;
   // Compute_nearest_data: 2S/surface.cpp:450-526 (targets of set t vs surface 1-t)
   for (int t = 0; t < 2; t++) {
     const int src = 1 - t;
     const Spheroid& S = cen[src];
-    CellIndex CI;
+    PointTree CI;
     CI.build(P[src]);
     const int n = (int)P[t].size();
     G->b[t].assign(n, 0.0);
@@ -586,11 +618,10 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
     G->i123[t].assign(3 * n, 0);
 #pragma omp parallel for schedule(dynamic, 64)
     for (int i = 0; i < n; i++) {
-      thread_local std::vector<double> d2c;
       const double* pt = P[t][i].x;
       int i1, i2, i3;
       monge(S, pt, i1, i2, i3);
-      int nrst_i = CI.nearest(P[src], pt, i3, d2c);
+      int nrst_i = CI.nearest(pt, i3);
       G->nrst[t][i] = nrst_i;
       if (nrst_i < 0) continue;
       double x0[3], n0[3];
@@ -610,6 +641,9 @@ extern "C" int hr_geom2s_generate(const hr_geom2s_params* prm, int N, hr_geom2s*
       }
       surface_force(S, prm->axes, x0, n0, &G->f0[t][3 * i], prm->tension_body != 0);
     }
+    t1 = omp_get_wtime();
+    G->phase_s[2 + t] = t1 - t0;
+    t0 = t1;
   }
   *out = G.release();
   return HR_OK;
@@ -639,6 +673,12 @@ extern "C" int hr_geom2s_view(const hr_geom2s* G, hr_scene2s* sc, const double**
   }
   sc->h = G->h;
   sc->delta = G->delta;
+  return HR_OK;
+}
+
+extern "C" int hr_geom2s_phase_seconds(const hr_geom2s* G, double* out4) {
+  if (!G || !out4) return HR_ERR_ARG;
+  for (int k = 0; k < 4; k++) out4[k] = G->phase_s[k];
   return HR_OK;
 }
 

@@ -327,6 +327,11 @@ int hr_geom2s_generate(const hr_geom2s_params* p, int N, hr_geom2s** out);
  * f = 2 H gamma n - grad_s gamma, gamma = 1 + z^2, at every quadrature point. */
 int hr_geom2s_view(const hr_geom2s* g, hr_scene2s* scene, const double** force);
 void hr_geom2s_destroy(hr_geom2s* g);
+/* Wall seconds of the set-up phases of hr_geom2s_generate: [0] quadrature
+ * points of both surfaces, [1] interfacial forces, [2] / [3] nearest data
+ * (nearest-point search, Newton projection, Monge patch, forces at the
+ * nearest points) of target sets 0 / 1. */
+int hr_geom2s_phase_seconds(const hr_geom2s* g, double* out4);
 
 /* ------------------------------------------------- learned warm start */
 /* No counterpart in the reference (its GMRES starts from zero,
