@@ -10,17 +10,18 @@ factors of the 7th-order kernels (2S/utilities.cpp:211-254 and :292-323) are
 
 where G1 = f1 / lam, G2 = f2 / lam^3, G3 = f3 / lam^5 are even in lam and
 therefore analytic in s = lam^2, with the reference's r -> 0 values
-(32/5, 256/15, 128/45) / sqrt(pi) as their limits at s = 0. Each G is
-represented on lam in [0, 8] (s in [0, 64], the smoothed branch) by NI pieces
-uniform in lam; piece i covers s in [(i w)^2, ((i+1) w)^2], w = 8 / NI, and is a
-degree-DEG polynomial in t = s - c_i about the centre c_i of the piece, the
-interpolant at DEG + 1 Chebyshev nodes of the piece widened by 1e-3 in lam at
-each end, solved in 80-digit arithmetic (mpmath). The script checks the
-rounded coefficients against the 80-digit function on a dense grid and
-writes the maximum relative error into the generated file (~1e-16 with
-64 pieces of degree 11). For the FP32 path it also writes float tables with
-pieces uniform in s (so the piece index needs no square root), checked by
-emulating their FP32 evaluation.
+(32/5, 256/15, 128/45) / sqrt(pi) as their limits at s = 0.
+
+FP64 tables (the FP64 sums): on s in [0, 64], pieces 0 .. NI centred on the
+grid c_i = i * 64 / NI, each a polynomial of degree DEG in t = s - c_i (the
+interpolant at DEG + 1 Chebyshev nodes of the piece, solved in 80-digit
+arithmetic with mpmath): G1 and G2 64 pieces of degree 13, G3 256 pieces of
+degree 9. A kernel finds the piece of s as round-to-nearest(s * NI / 64) with
+one fused multiply-add and needs no stored centre. The script checks the
+rounded coefficients against the 80-digit function and writes the maximum
+relative error into the generated file (~1e-16). FP32 tables (the
+reduced-precision path): pieces uniform in s with the piece index floor(s *
+NI32 / 64), checked by emulating their FP32 evaluation.
 
 Run from this directory: python gen_smoothing_tables.py
 """
@@ -29,9 +30,6 @@ import os
 import mpmath as mp
 
 mp.mp.dps = 80
-NI = 64
-DEG = 11
-LAM_MAX = 8
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
@@ -60,50 +58,11 @@ def G3(s):
     return (mp.erf(lam) + (-1 - mp.mpf(2) / 3 * s + mp.mpf(52) / 45 * s * s - mp.mpf(8) / 45 * s ** 3) * E(lam)) / lam ** 5
 
 
-def piece(f, i):
-    """Monomial coefficients (in t = s - c) and centre c of piece i: the
-    polynomial interpolating f at DEG + 1 Chebyshev nodes of the widened piece,
-    solved in 80-digit arithmetic."""
-    w = mp.mpf(LAM_MAX) / NI
-    lo, hi = mp.mpf(i) * w, mp.mpf(i + 1) * w
-    slo = mp.mpf(0) if i == 0 else (lo - mp.mpf("1e-3")) ** 2
-    shi = (hi + mp.mpf("1e-3")) ** 2
-    c = (lo * lo + hi * hi) / 2
-    half, mid = (shi - slo) / 2, (shi + slo) / 2
-    n = DEG + 1
-    ts = [mid + half * mp.cos(mp.pi * (k + mp.mpf(1) / 2) / n) - c for k in range(n)]
-    V = mp.matrix(n, n)
-    for r, t in enumerate(ts):
-        for j in range(n):
-            V[r, j] = t ** j
-    vals = mp.matrix([f(t + c) for t in ts])
-    coef = mp.lu_solve(V, vals)
-    return [coef[j] for j in range(n)], c, (lo, hi)
-
-
 def horner(coef, t):
     p = mp.mpf(0)
     for a in reversed(coef):
         p = p * t + a
     return p
-
-
-def build(f):
-    """Rounded pieces and the worst relative error of the rounded coefficients
-    (evaluated exactly) over 41 points per piece."""
-    out, worst = [], mp.mpf(0)
-    for i in range(NI):
-        coef, c, (lo, hi) = piece(f, i)
-        cd = [float(a) for a in coef]
-        cc = float(c)
-        for k in range(41):
-            lam = lo + (hi - lo) * k / 40
-            s = mp.mpf(float(lam * lam))
-            approx = horner([mp.mpf(a) for a in cd], s - mp.mpf(cc))
-            exact = f(s)
-            worst = max(worst, abs(approx - exact) / abs(exact))
-        out.append((cc, cd))
-    return out, worst
 
 
 # FP64 tables centred on a uniform grid in s, for an index formed by one
@@ -196,20 +155,9 @@ def build32(f):
 
 def main():
     lines = ["// Generated by gen_smoothing_tables.py; do not edit.",
-             "// Piecewise polynomials G(s), s = (r/delta)^2 in [0, 64], of the on-surface",
-             "// smoothing factors: %d pieces uniform in r/delta, degree %d in t = s - centre." % (NI, DEG),
-             "// Per piece: centre, then coefficients of t^0 .. t^%d." % DEG,
+             "// Piecewise polynomials G(s), s = (r/delta)^2 in [0, 64], of the on-surface smoothing factors.",
+             "// FP64: pieces centred on a uniform grid in s, monomial coefficients in t = s - centre.",
              "// The includer defines HR_SMOOTH_STORAGE (e.g. static __device__ const)."]
-    lines.append("#define HR_SMOOTH_PIECES %d" % NI)
-    lines.append("#define HR_SMOOTH_DEG %d" % DEG)
-    for name, f in (("G1", G1), ("G2", G2), ("G3", G3)):
-        tab, worst = build(f)
-        lines.append("// %s: max relative error of the rounded coefficients (exact arithmetic) %.2e" % (name, float(worst)))
-        print(name, "max rel err", float(worst))
-        lines.append("HR_SMOOTH_STORAGE double kSmooth%s[%d * %d] = {" % (name, NI, DEG + 2))
-        for c, cd in tab:
-            lines.append("    " + ", ".join(repr(v) for v in [c] + cd) + ",")
-        lines.append("};")
     for name, f in (("G1", G1), ("G2", G2), ("G3", G3)):
         ni, deg = GRID_TABLES[name]
         tab, worst = build_grid(f, ni, deg)

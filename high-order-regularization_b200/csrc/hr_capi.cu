@@ -1159,6 +1159,12 @@ extern "C" int hr_plan2s_work(hr_plan2s* plan, int which, hr_work* w) {
     DBuf<double> tmp;
     tmp.alloc(plan->n);
     const Batch* B;
+    // one counting launch of the batch (ordinary launches skip the counts)
+    struct Counting {
+      Ctx& C;
+      explicit Counting(Ctx& c) : C(c) { C.count_work = true; }
+      ~Counting() { C.count_work = false; }
+    } counting(*plan->C);
     if (which == 0) {
       HR_CHECK_CUDA(cudaMemsetAsync(tmp.p, 0, sizeof(double) * plan->n, st));
       plan_matvec(*plan, tmp.p, tmp.p, 0);

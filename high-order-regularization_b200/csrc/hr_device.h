@@ -67,10 +67,11 @@ enum Family : int { F_SL = 0, F_DL = 1, F_E2G = 2 };
 // on-surface tasks, or the extend-to-grid box-face sums) in one launch on st,
 // the rest in another on `side` (forked from and joined back to st with the
 // two events; on st as well when side is null) — then reduces the partial sums
-// per target (deterministic order) and applies the epilogue.
+// per target (deterministic order) and applies the epilogue. With count, the
+// FP64 launches also add their per-branch pair counts to the tasks' counters.
 void launch_eval(int family, const EvalTask* d_tasks, const BlockRef* d_items, const Seg* d_segs,
                  int nitems, int n_on, int ntask_blocks, const int2* d_task_blocks, cudaStream_t st,
-                 cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, bool mixed);
+                 cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, bool mixed, bool count);
 
 // Upward pass: proxy moments of every non-root node of a tree.
 struct MomItem {

@@ -440,7 +440,7 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
 
 void Batch::launch(Ctx& C) {
   launch_eval(family, d_tasks.p, d_items.p, d_segs.p, nitems, n_on, ntask_blocks, d_task_blocks.p,
-              C.stream, C.side, C.ev_fork, C.ev_join, !tasks.empty() && tasks[0].mixed);
+              C.stream, C.side, C.ev_fork, C.ev_join, !tasks.empty() && tasks[0].mixed, C.count_work);
   C.launches += 1 + (n_on > 0 ? 1 : 0) + (nitems > n_on ? 1 : 0);
 }
 

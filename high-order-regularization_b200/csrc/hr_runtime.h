@@ -92,6 +92,9 @@ struct Ctx {
   std::string err;
   long long launches = 0;
   int num_sms = 148;
+  // while set, FP64 boundary-sum launches record their per-branch pair counts
+  // (the tasks' work counters); other launches skip the tests
+  bool count_work = false;
   DBuf<unsigned long long> counters;  // [0] reg pairs [1] plain pairs [2] proxies
   DBuf<int> tc_err;                   // set by a tensor-core kernel whose bounded wait ran out
   // two pinned host buffers of kPinChunk bytes for staged reads (d2h_staged),
