@@ -1101,294 +1101,6 @@ __global__ void __launch_bounds__(kTB2, 8) eval_kernel_on2(const EvalTask* __res
   else run_item_on2<K_DL_ON>(sT, it, segs, sm, sf, chebf, stab32);
 }
 
-// ------------------------------------------ two targets per thread (FP64, on-surface)
-
-// One FP64 on-surface pair (Call_Ds_SL_onSurf / Call_Ds_DL_onSurf,
-// 2S/KITC.cpp:807-846, 921-957, with the tabulated smoothing factors of
-// pair64) from source values already in registers: (x, y, z), area x normal
-// and, for the Stokeslet, area x density (the stresslet's density is not
-// area-weighted). Returns the reference's branch (r <= 8 delta, r >= 1e-14)
-// for the work counters.
-template <int KIND>
-__device__ __forceinline__ bool pair64_on(double Xj, double Yj, double Zj, double NXj, double NYj, double NZj,
-                                          double QXj, double QYj, double QZj, double px, double py, double pz,
-                                          const double* q0, const Reg& g, const double* __restrict__ stab,
-                                          double& a0, double& a1, double& a2) {
-  const double dx = px - Xj, dy = py - Yj, dz = pz - Zj;
-  const double r2 = dx * dx + dy * dy + dz * dz;
-  if (KIND == K_SL_ON) {
-    const double fx = QXj - q0[0] * NXj;
-    const double fy = QYj - q0[0] * NYj;
-    const double fz = QZj - q0[0] * NZj;
-    const double fdd = fx * dx + fy * dy + fz * dz;
-    double H1, H2;
-    if (r2 > g.dplain) {
-      const double ri = rsqrt(r2);
-      H1 = ri;
-      H2 = ri * ri * ri;
-    } else {
-      double t;
-      const int i = smooth_piece<TabG1::kPieces>(r2 * g.inv_d2, t);
-      H1 = smooth_horner<TabG1>(stab, i, t);
-      H2 = smooth_horner<TabG2>(stab + TabG1::kLen, i, t);
-    }
-    H2 *= fdd;
-    a0 += fx * H1 + dx * H2;
-    a1 += fy * H1 + dy * H2;
-    a2 += fz * H1 + dz * H2;
-  } else {
-    const double gx = QXj - q0[0];
-    const double gy = QYj - q0[1];
-    const double gz = QZj - q0[2];
-    const double gdd = gx * dx + gy * dy + gz * dz;
-    const double ndd = NXj * dx + NYj * dy + NZj * dz;
-    double H3;
-    if (r2 > g.dplain) {
-      const double ri = rsqrt(r2), ri2 = ri * ri;
-      H3 = ri2 * ri2 * ri;
-    } else {
-      double t;
-      const int i = smooth_piece<TabG3::kPieces>(r2 * g.inv_d2, t);
-      H3 = smooth_horner<TabG3>(stab, i, t);
-    }
-    const double kernel = ndd * gdd * H3;
-    a0 += dx * kernel;
-    a1 += dy * kernel;
-    a2 += dz * kernel;
-  }
-  return r2 <= g.d64 && r2 >= g.r0sq;
-}
-
-// FP64 proxies of a run of Chebyshev rows for two targets (each shared-memory
-// read of a proxy's moments serves both); the arithmetic of proxies64_rows.
-template <bool DL>
-__device__ __forceinline__ void proxies64_rows2(const double2* __restrict__ s2, int row0, int nrows, int P1,
-                                                const double* __restrict__ cheb, const double (&px)[2][3],
-                                                const double (&q0)[2][3], double (&acc)[2][3]) {
-  constexpr int W = DL ? 5 : 3;  // double2 per proxy
-  for (int r = 0; r < nrows; r++) {
-    const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
-    const double cx = cheb[pi], cy = cheb[P1 + pj];
-    double d0[2], d1[2], r01[2], g0r[2];
-#pragma unroll
-    for (int q = 0; q < 2; q++) {
-      d0[q] = px[q][0] - cx;
-      d1[q] = px[q][1] - cy;
-      r01[q] = d0[q] * d0[q] + d1[q] * d1[q];
-      g0r[q] = q0[q][0] * d0[q] + q0[q][1] * d1[q];
-    }
-    const double2* row = s2 + r * P1 * W;
-    for (int pk = 0; pk < P1; pk++) {
-      const double cz = cheb[2 * P1 + pk];
-      const double2* m = row + pk * W;
-      if (DL) {
-        const double2 s01 = m[0], s23 = m[1], s45 = m[2], n01 = m[3], n2 = m[4];
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-          const double d2 = px[q][2] - cz;
-          const double rinv = rsqrt(fma(d2, d2, r01[q]));
-          const double dmd = s01.x * (d0[q] * d0[q]) + s01.y * (d1[q] * d1[q]) + s23.x * (d2 * d2) +
-                             s23.y * (d0[q] * d1[q]) + s45.x * (d0[q] * d2) + s45.y * (d1[q] * d2);
-          const double mnd = n01.x * d0[q] + n01.y * d1[q] + n2.x * d2;
-          const double g0d = fma(q0[q][2], d2, g0r[q]);
-          const double ri2 = rinv * rinv;
-          const double kernel = (dmd - g0d * mnd) * (ri2 * ri2 * rinv);
-          acc[q][0] += d0[q] * kernel;
-          acc[q][1] += d1[q] * kernel;
-          acc[q][2] += d2 * kernel;
-        }
-      } else {
-        const double2 m01 = m[0], m23 = m[1], m45 = m[2];
-#pragma unroll
-        for (int q = 0; q < 2; q++) {
-          const double d2 = px[q][2] - cz;
-          const double rinv = rsqrt(fma(d2, d2, r01[q]));
-          const double f0n0 = q0[q][0];
-          const double m0 = m01.x - f0n0 * m23.y;
-          const double m1 = m01.y - f0n0 * m45.x;
-          const double m2 = m23.x - f0n0 * m45.y;
-          const double temp = (m0 * d0[q] + m1 * d1[q] + m2 * d2) * (rinv * rinv * rinv);
-          acc[q][0] += m0 * rinv + temp * d0[q];
-          acc[q][1] += m1 * rinv + temp * d1[q];
-          acc[q][2] += m2 * rinv + temp * d2;
-        }
-      }
-    }
-  }
-}
-
-// The FP64 on-surface items (K_SL_ON / K_DL_ON) with two targets per thread:
-// a CTA of kTB2 = 64 threads covers the block's 128 targets (warp w holds
-// targets 64 w + lane and 64 w + 32 + lane, mask words 2 w and 2 w + 1), so
-// every source and proxy read from shared memory serves two pairs and each
-// thread carries two independent chains of FP64 work.
-template <int KIND, bool COUNT>
-__device__ __forceinline__ void run_item_on2_64(const EvalTask& T, const BlockRef& it, const Seg* __restrict__ segs,
-                                                double* sm, double* cheb, const double* stab) {
-  constexpr bool DL = (KIND == K_DL_ON);
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int blk = it.blk;
-  double px[2][3], q0[2][3];
-  bool valid[2];
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    const int k = blk * kTB + warp * 64 + q * 32 + lane;
-    valid[q] = k < T.nt;
-    const int t = valid[q] ? T.tord[k] : 0;
-    for (int c = 0; c < 3; c++) px[q][c] = valid[q] ? T.txyz[3 * t + c] : 0.0;
-    if (DL) {
-      for (int c = 0; c < 3; c++) q0[q][c] = valid[q] ? T.tq[3 * t + c] : 0.0;
-    } else {
-      // f0_dot_n0 = Surfc[i].f . Surfc[i].Nrml  (2S/KITC.cpp:1461)
-      q0[q][0] = valid[q] ? T.tq[3 * t] * T.tnrm[3 * t] + T.tq[3 * t + 1] * T.tnrm[3 * t + 1] +
-                                T.tq[3 * t + 2] * T.tnrm[3 * t + 2]
-                          : 0.0;
-      q0[q][1] = q0[q][2] = 0.0;
-    }
-  }
-  const Reg g = make_reg(T.DEL);
-  double a[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-  unsigned long long creg = 0, cplain = 0, cprox = 0;
-  double* wsm = sm + warp * kWarpSm;
-  double* wcheb = cheb + warp * 3 * kMaxP1;
-  for (int qs = it.seg0; qs < it.seg1; qs++) {
-    const Seg sg = segs[qs];
-    const Entry E = T.entries[sg.entry];
-    const uint32_t mA = E.mask[2 * warp], mB = E.mask[2 * warp + 1];
-    if ((mA | mB) == 0u) continue;
-    const bool actA = valid[0] && ((mA >> lane) & 1u);
-    const bool actB = valid[1] && ((mB >> lane) & 1u);
-    if (E.type == 1) {
-      const int m0 = sg.s0, m1 = sg.s1 - 1;
-      for (int s0 = m0; s0 <= m1; s0 += kNT) {
-        const int cnt = min(kNT, m1 - s0 + 1);
-        __syncwarp();
-        for (int i = lane; i < cnt; i += 32) {
-          const int s = s0 + i;
-          const double as = T.sa[s];
-          const double aq = DL ? 1.0 : as;
-          double2* w2 = reinterpret_cast<double2*>(wsm) + 5 * i;
-          w2[0] = make_double2(T.sx[s], T.sy[s]);
-          w2[1] = make_double2(T.sz[s], as);
-          w2[2] = make_double2(as * T.snx[s], as * T.sny[s]);
-          w2[3] = make_double2(as * T.snz[s], aq * T.qx[s]);
-          w2[4] = make_double2(aq * T.qy[s], aq * T.qz[s]);
-        }
-        __syncwarp();
-        if (!actA && !actB) continue;
-        double pA[3] = {0.0, 0.0, 0.0}, pB[3] = {0.0, 0.0, 0.0};
-        unsigned crA = 0, crB = 0;
-#pragma unroll 2
-        for (int j = 0; j < cnt; j++) {
-          const double2* s2 = reinterpret_cast<const double2*>(wsm) + 5 * j;
-          const double2 v0 = s2[0], v1 = s2[1], v2 = s2[2], v3 = s2[3], v4 = s2[4];
-          crA += pair64_on<KIND>(v0.x, v0.y, v1.x, v2.x, v2.y, v3.x, v3.y, v4.x, v4.y, px[0][0], px[0][1],
-                                 px[0][2], q0[0], g, stab, pA[0], pA[1], pA[2]);
-          crB += pair64_on<KIND>(v0.x, v0.y, v1.x, v2.x, v2.y, v3.x, v3.y, v4.x, v4.y, px[1][0], px[1][1],
-                                 px[1][2], q0[1], g, stab, pB[0], pB[1], pB[2]);
-        }
-        if (actA)
-          for (int c = 0; c < 3; c++) a[0][c] += pA[c];
-        if (actB)
-          for (int c = 0; c < 3; c++) a[1][c] += pB[c];
-        if (COUNT) {
-          if (actA) {
-            creg += crA;
-            cplain += cnt - crA;
-          }
-          if (actB) {
-            creg += crB;
-            cplain += cnt - crB;
-          }
-        }
-      }
-    } else {
-      // far node: the proxy-major FP64 moments through the warp's tile, double-buffered
-      const int P1 = T.P1, Pf = T.Pf, C = T.C;
-      constexpr int kBpp = DL ? 80 : 48;  // bytes per proxy
-      constexpr int kHalf = kWarpSm * 4;  // bytes per buffer
-      const char* src = reinterpret_cast<const char*>(T.mom + (size_t)E.node * Pf * C);
-      char* buf = reinterpret_cast<char*>(wsm);
-      const int rowb = P1 * kBpp;
-      const int nr = max(1, kHalf / rowb);
-      const int nrow_all = P1 * P1;
-      const int nch = (nrow_all + nr - 1) / nr;
-      __syncwarp();
-      for (int i = lane; i < 3 * P1; i += 32) wcheb[i] = T.tcheb[(size_t)E.node * 3 * P1 + i];
-      warp_copy_async(buf, src, min(nr, nrow_all) * rowb, lane);
-      double acc[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
-      for (int ch = 0; ch < nch; ch++) {
-        const int row0 = ch * nr, rows = min(nr, nrow_all - row0);
-        if (ch + 1 < nch) {
-          const int r1 = row0 + nr;
-          warp_copy_async(buf + ((ch + 1) & 1) * kHalf, src + (size_t)r1 * rowb, min(nr, nrow_all - r1) * rowb,
-                          lane);
-          copy_async_wait<1>();
-        } else {
-          copy_async_wait<0>();
-        }
-        __syncwarp();
-        if (actA || actB)
-          proxies64_rows2<DL>(reinterpret_cast<const double2*>(buf + (ch & 1) * kHalf), row0, rows, P1, wcheb, px,
-                              q0, acc);
-        __syncwarp();
-      }
-      if (actA)
-        for (int c = 0; c < 3; c++) a[0][c] += acc[0][c];
-      if (actB)
-        for (int c = 0; c < 3; c++) a[1][c] += acc[1][c];
-      if (COUNT) cprox += (unsigned long long)Pf * ((actA ? 1 : 0) + (actB ? 1 : 0));
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < 2; q++) {
-    double* o = T.partial + ((size_t)it.slot * kTB + warp * 64 + q * 32 + lane) * 3;
-    o[0] = a[q][0];
-    o[1] = a[q][1];
-    o[2] = a[q][2];
-  }
-  if (COUNT && T.counters) {
-    for (int off = 16; off > 0; off >>= 1) {
-      creg += __shfl_down_sync(0xffffffffu, creg, off);
-      cplain += __shfl_down_sync(0xffffffffu, cplain, off);
-      cprox += __shfl_down_sync(0xffffffffu, cprox, off);
-    }
-    if (lane == 0) {
-      if (creg) atomicAdd(&T.counters[0], creg);
-      if (cplain) atomicAdd(&T.counters[1], cplain);
-      if (cprox) atomicAdd(&T.counters[3], cprox);
-    }
-  }
-}
-
-template <int FAM, bool COUNT>
-__global__ void __launch_bounds__(kTB2, 6) eval_kernel_on2_64(const EvalTask* __restrict__ tasks,
-                                                              const BlockRef* __restrict__ items,
-                                                              const Seg* __restrict__ segs) {
-  constexpr int kW2 = kTB2 / 32;
-  __shared__ __align__(16) double sm[kW2 * kWarpSm];
-  __shared__ double cheb[kW2 * 3 * kMaxP1];
-  __shared__ EvalTask sT;
-  __shared__ __align__(16) double stab[FAM == F_SL ? TabG1::kLen + TabG2::kLen : TabG3::kLen];
-  const BlockRef it = items[blockIdx.x];
-  if (threadIdx.x == 0) sT = tasks[it.task];
-  {
-    // the FP64 tables with the powers of 1/delta folded in (as in eval_kernel)
-    const Reg gs = make_reg(tasks[it.task].DEL);
-    if (FAM == F_SL) {
-      for (int i = threadIdx.x; i < TabG1::kLen; i += blockDim.x) {
-        stab[i] = kSmoothSG1[i] * gs.inv_d;
-        stab[TabG1::kLen + i] = kSmoothSG2[i] * gs.inv_d3;
-      }
-    } else {
-      for (int i = threadIdx.x; i < TabG3::kLen; i += blockDim.x) stab[i] = kSmoothSG3[i] * gs.inv_d5;
-    }
-  }
-  __syncthreads();
-  if (FAM == F_SL) run_item_on2_64<K_SL_ON, COUNT>(sT, it, segs, sm, cheb, stab);
-  else run_item_on2_64<K_DL_ON, COUNT>(sT, it, segs, sm, cheb, stab);
-}
-
 // ON = true: the batch's lean items only — on-surface kinds (K_SL_ON / K_DL_ON)
 // or, for the extend-to-grid family, the plain box-face sums (K_E2G_*_AWAY).
 // Their code path needs fewer registers than the others' (no nearest-point
@@ -1526,8 +1238,6 @@ void launch_family(const EvalTask* d_tasks, const BlockRef* d_items, const Seg* 
   }
   if (n_on > 0) {
     if constexpr (MIXED && FAM != F_E2G) eval_kernel_on2<FAM><<<n_on, kTB2, 0, st>>>(d_tasks, d_items, d_segs);
-    else if constexpr (FAM != F_E2G)
-      eval_kernel_on2_64<FAM, COUNT><<<n_on, kTB2, 0, st>>>(d_tasks, d_items, d_segs);
     else eval_kernel<FAM, MIXED, true, COUNT><<<n_on, kTB, 0, st>>>(d_tasks, d_items, d_segs);
   }
   if (nitems > n_on)

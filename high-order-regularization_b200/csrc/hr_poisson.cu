@@ -327,6 +327,195 @@ __global__ void __launch_bounds__(kDstThreads, 4)
   }
 }
 
+// ------------------------------------------------------------------------
+// Register DST-I pass for lines of n = 64 R - 1 points (N = 64 R, complex
+// length P = 32 R; R = 2, 3, 4, 6, 8: the N = 384 grid is R = 6): one warp
+// per line, the complex sequence held as R values per lane (element
+// m = 32 a + b in register a of lane b), so the FFT runs in registers and
+// warp shuffles and shared memory only stages the rotated store.
+//   1. y_j of the auxiliary-array method, read straight from global memory
+//      (lane b needs x_{j}, x_{j+1} and their mirrors for j = 64 a + 2 b);
+//   2. P = R x 32: an R-point DFT over each lane's registers, the twiddles
+//      W_P^{b k1}, then a 32-point decimation-in-frequency DFT across the
+//      lanes (five butterfly stages with shuffles), leaving Z_{k1 + R k2} in
+//      register k1 of lane bitrev5(k2);
+//   3. the real split with the partner Z_{P-k} fetched by one shuffle per
+//      register (lane b ^ 31 for k1 > 0), and the odd-output recurrence as an
+//      in-lane prefix over k1 plus a warp scan over k2;
+//   4. the CTA's kDstLines lines written rotated through shared memory with
+//      the pass's epilogue, as in dst_pass_kernel.
+
+__device__ __forceinline__ void dft6(double2* v) {
+  // 6 = 2 x 3: DFTs of the even and the odd elements, then W6^k
+  double2 e0 = v[0], e1 = v[2], e2 = v[4], o0 = v[1], o1 = v[3], o2 = v[5];
+  dft3(e0, e1, e2);
+  dft3(o0, o1, o2);
+  const double h = 0.86602540378443864676;  // sin(pi / 3)
+  const double2 t1 = make_double2(0.5 * o1.x + h * o1.y, 0.5 * o1.y - h * o1.x);    // e^{-i pi/3} o1
+  const double2 t2 = make_double2(-0.5 * o2.x + h * o2.y, -0.5 * o2.y - h * o2.x);  // e^{-2i pi/3} o2
+  v[0] = cadd(e0, o0);
+  v[3] = csub(e0, o0);
+  v[1] = cadd(e1, t1);
+  v[4] = csub(e1, t1);
+  v[2] = cadd(e2, t2);
+  v[5] = csub(e2, t2);
+}
+
+template <int R>
+__device__ __forceinline__ void dft_regs(double2* v) {
+  if constexpr (R == 2) dft2(v[0], v[1]);
+  else if constexpr (R == 3) dft3(v[0], v[1], v[2]);
+  else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3]);
+    // dft4 leaves outputs in order 0, 1, 2, 3 (a0, a1, a2, a3)
+  } else if constexpr (R == 6) dft6(v);
+  else dft8(v);
+}
+
+__device__ __forceinline__ int brev5(int x) { return (int)(__brev((unsigned)x) >> 27); }
+
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+template <int R>
+__global__ void __launch_bounds__(kDstThreads, 3)
+    dst_pass_reg_kernel(int, DstRadix, const double* __restrict__ in, double* __restrict__ out, int mode,
+                        const double2* __restrict__ tw, const double* __restrict__ sintab,
+                        const double* __restrict__ evc, const double* __restrict__ evs, double scale,
+                        const double* __restrict__ w, double* __restrict__ u) {
+  extern __shared__ __align__(16) double dsm[];
+  constexpr int T = kDstLines;
+  constexpr int RS = T + 1;
+  constexpr int P = 32 * R, N = 2 * P, n = N - 1;
+  static_assert(kDstThreads == 32 * T, "one warp per line");
+  const long lines = (long)n * n;
+  const long l0 = (long)blockIdx.x * T;
+  const int nt = (int)min((long)T, lines - l0);
+  const int t = threadIdx.x >> 5, b = threadIdx.x & 31;
+  const bool live = t < nt;
+
+  // 1. z_m = y_{2m} + i y_{2m+1}, m = 32 a + b
+  double2 z[R];
+  {
+    const double* row = in + (l0 + (live ? t : 0)) * n;
+#pragma unroll
+    for (int a = 0; a < R; a++) {
+      const int j = 64 * a + 2 * b;
+      double yr = 0.0, yi = 0.0;
+      if (live) {
+        if (j > 0) {
+          const double xj = row[j - 1], xm = row[N - j - 1];
+          yr = __ldg(&sintab[j]) * (xj + xm) + 0.5 * (xj - xm);
+        }
+        const double xj1 = row[j], xm1 = row[N - j - 2];
+        yi = __ldg(&sintab[j + 1]) * (xj1 + xm1) + 0.5 * (xj1 - xm1);
+      }
+      z[a] = make_double2(yr, yi);
+    }
+  }
+
+  // 2. Z_{k1 + R k2} = sum_b W32^{b k2} W_P^{b k1} sum_a z_{32 a + b} W_R^{a k1}
+  dft_regs<R>(z);
+#pragma unroll
+  for (int k1 = 1; k1 < R; k1++) z[k1] = cmul(z[k1], __ldg(&tw[2 * b * k1]));  // W_P^x = tw[2x]
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool upper = (b & s) != 0;
+    const double sg = upper ? -1.0 : 1.0;
+    // W_{2s}^{i}, i = b mod s, for the upper lanes; 1 for the lower ones
+    const double2 wt = (s > 1 && upper) ? __ldg(&tw[(b & (s - 1)) * (N / (2 * s))]) : make_double2(1.0, 0.0);
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) {
+      const double2 p = make_double2(__shfl_xor_sync(0xffffffffu, z[k1].x, s),
+                                     __shfl_xor_sync(0xffffffffu, z[k1].y, s));
+      const double2 q = make_double2(fma(sg, z[k1].x, p.x), fma(sg, z[k1].y, p.y));  // lower: p + z; upper: p - z
+      z[k1] = s > 1 ? cmul(q, wt) : q;
+    }
+  }
+  // lane b now holds Z_k, k = k1 + R k2 with k2 = bitrev5(b)
+  const int k2 = brev5(b);
+
+  // 3. real split: partner Z_{P - k}: k1 > 0 -> register R - k1 of lane b ^ 31;
+  //    k1 = 0 -> register 0 of lane bitrev5((32 - k2) mod 32)
+  double ev[R], od[R];
+  {
+    const int src0 = brev5((32 - k2) & 31);
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) {
+      const double2 a = z[k1];
+      const double2 c = k1 == 0 ? shfl2(z[0], src0) : shfl2(z[R - k1], b ^ 31);
+      const int k = k1 + R * k2;
+      if (k == 0) {
+        ev[k1] = a.x + a.y;  // R_0
+        od[k1] = 0.0;
+      } else {
+        const double Ex = 0.5 * (a.x + c.x), Ey = 0.5 * (a.y - c.y);
+        const double Ox = 0.5 * (a.y + c.y), Oy = -0.5 * (a.x - c.x);
+        const double2 wk = __ldg(&tw[k]);
+        const double Yx = Ex + (wk.x * Ox - wk.y * Oy);
+        const double Yy = Ey + (wk.x * Oy + wk.y * Ox);
+        ev[k1] = 2.0 * Yx;  // summed into the even outputs below
+        od[k1] = -2.0 * Yy; // output 2k - 1
+      }
+    }
+  }
+  // even outputs: 2F at 2k = R_0 + sum_{k' = 1..k} 2 Yx_{k'} (natural order k = k1 + R k2)
+  {
+#pragma unroll
+    for (int k1 = 1; k1 < R; k1++) ev[k1] += ev[k1 - 1];
+    double incl = ev[R - 1];
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const double x = __shfl_sync(0xffffffffu, incl, brev5((k2 - d) & 31));
+      if (k2 >= d) incl += x;
+    }
+    const double excl = incl - ev[R - 1];
+#pragma unroll
+    for (int k1 = 0; k1 < R; k1++) ev[k1] += excl;
+  }
+  // stage this line's outputs for the rotated store: output 2k (even), 2k - 1 (odd)
+  double* tile = dsm;
+#pragma unroll
+  for (int k1 = 0; k1 < R; k1++) {
+    const int k = k1 + R * k2;
+    tile[(2 * k) * RS + t] = ev[k1];
+    if (k > 0) tile[(2 * k - 1) * RS + t] = od[k1];
+  }
+  __syncthreads();
+
+  // 4. rotated stores with the pass's epilogue (as dst_pass_kernel)
+  for (int idx = threadIdx.x; idx < n * T; idx += kDstThreads) {
+    const int kk = idx / T, tt = idx - kk * T;
+    if (tt >= nt) continue;
+    const long l = l0 + tt;
+    const double F2 = tile[kk * RS + tt];
+    if (mode == 0) {
+      out[kk * lines + l] = F2;
+    } else if (mode == 3) {
+      out[kk * lines + l] = F2 * scale;
+    } else {
+      const int ja = (int)(l / n), jb = (int)(l - (long)ja * n);
+      if (mode == 1) {
+        const double c1 = __ldg(&evc[kk]), s1 = __ldg(&evs[kk]);
+        const double ca = __ldg(&evc[ja]), sa = __ldg(&evs[ja]);
+        const double cb = __ldg(&evc[jb]), sb = __ldg(&evs[jb]);
+        const double lap7 = s1 + sa + sb;
+        const double sum8 = c1 * ca * cb;
+        const double factor = 2.0 / 3.0 * (2.0 * lap7 + sum8 - 1.0);
+        double v = F2;
+        if (fabs(factor) > 1.e-14) v /= factor;
+        else v = 0.0;
+        out[kk * lines + l] = v;
+      } else {
+        const long M = n + 2;  // grid size N_grid + 1
+        const long gi = ((long)(kk + 1) * M + (ja + 1)) * M + (jb + 1);
+        u[gi] = w[gi] + F2 * scale;
+      }
+    }
+  }
+}
+
 // Transfinite (Coons) extension of the boundary values (extend_into_cube,
 // E2G/main.cpp:1494-1527):
 //   G = F - E1 - E2 - E3 + C,  F = x g(N,j,k) + (1-x) g(0,j,k) + y g(i,N,k)
@@ -475,12 +664,19 @@ struct DstPlan {
       rad.r[rad.nst++] = f;
       q /= f;
     }
-    smem = 2 * (size_t)dst_bufd(P) * sizeof(double);
+    // lines of 64 R - 1 points (R = 2, 3, 4, 6, 8; the N = 384 grid) run the
+    // register pass; the other benchmark sizes (N = 48, 96) passes compiled
+    // for their line length; any other the general shared-memory pass
+    const int R = P % 32 == 0 ? P / 32 : 0;
+    if (R == 2 || R == 3 || R == 4 || R == 6 || R == 8) {
+      fn = R == 2 ? dst_pass_reg_kernel<2> : R == 3 ? dst_pass_reg_kernel<3> : R == 4 ? dst_pass_reg_kernel<4>
+         : R == 6 ? dst_pass_reg_kernel<6> : dst_pass_reg_kernel<8>;
+      smem = (size_t)n * (kDstLines + 1) * sizeof(double);
+    } else {
+      fn = P == 48 ? dst_pass_kernel<48> : P == 24 ? dst_pass_kernel<24> : dst_pass_kernel<0>;
+      smem = 2 * (size_t)dst_bufd(P) * sizeof(double);
+    }
     HR_REQUIRE(smem <= 227 * 1024, "DST-I line longer than one CTA's shared memory holds");
-    // the grid sizes of the benchmark workloads (N = 48, 96, 384) run passes
-    // compiled for their line length
-    fn = P == 192 ? dst_pass_kernel<192> : P == 48 ? dst_pass_kernel<48> : P == 24 ? dst_pass_kernel<24>
-                                                                                    : dst_pass_kernel<0>;
     HR_CHECK_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     tmp.alloc((size_t)n * n * n);
     // twiddles e^{-2 pi i k/N} and sin(j pi/N), evaluated in extended precision

@@ -105,6 +105,7 @@ def lib():
         L.hr_geom2s_destroy.restype = None
         L.hr_plan2s_destroy.restype = None
         L.hr_ctx_destroy.restype = None
+        L.hr_dst1_plan_destroy.restype = None
         _lib = L
     return _lib
 
@@ -311,6 +312,20 @@ class Context:
         a = _f64(f).copy()
         self._check(lib().hr_dst_poisson3d(self.p, n, _dp(a)))
         return a
+
+    def dst1_3d(self, n, f):
+        """The plain 3D DST-I (FFTW's RODFT00 on all three axes, unnormalised) of
+        a row-major n^3 array, through a reusable plan (hr_dst1_*)."""
+        L = lib()
+        plan = ctypes.c_void_p()
+        self._check(L.hr_dst1_plan_create(self.p, n, ctypes.byref(plan)))
+        a = _f64(f)
+        out = np.empty_like(a)
+        try:
+            self._check(L.hr_dst1_execute(plan, _dp(a), _dp(out)))
+        finally:
+            L.hr_dst1_plan_destroy(plan)
+        return out
 
     def solve_poisson(self, N, L, band2, outside, p, u, variable):
         band2 = np.ascontiguousarray(band2, np.uint8)

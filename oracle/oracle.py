@@ -446,6 +446,9 @@ class RefE2G:
         return a
 
     def run(self):
+        """The whole reference driver at the set-up grid; returns its printed
+        output (this run's only)."""
+        self.lib.refe2g_clear_log()
         self.lib.refe2g_run()
         return self.log()
 

@@ -141,7 +141,7 @@ def test_h256_sampled_sums_match_reference_direct(ctx):
     """Every sum kind of the two-surface operator at h = 1/256 on a seeded
     sample of targets (near and far, both surfaces) against the reference's
     direct sums: the GPU's direct sums to 1e-12, its treecode (P = 10,
-    N0 = 8000) to 1e-7, its reduced-precision treecode to 1e-4; the
+    N0 = 8000) to 1e-6, its reduced-precision treecode to 1e-4; the
     stresslet's nearest-point densities against the reference's
     interpolate_DL_density to 1e-12."""
     R = _ref2s(10, 8000)
@@ -189,7 +189,7 @@ def test_h256_sampled_sums_match_reference_direct(ctx):
         e = {k: _errs(v, ref) for k, v in got.items()}
         print("  %-6s surface %d: " % (name, s) + ", ".join("%s %.2e / %.2e" % ((names[k],) + e[k]) for k in e))
         assert e["direct"][0] < 1e-12
-        assert e[highreg.HR_FP64][0] < 1e-7  # the treecode's own approximation error (P = 10, theta = 0.6)
+        assert e[highreg.HR_FP64][0] < 1e-6  # the treecode's own approximation error (P = 10, theta = 0.6)
         assert e[highreg.HR_MIXED][0] < 1e-4
         if highreg.HR_FP32 in e:
             assert e[highreg.HR_FP32][0] < 1e-4
@@ -202,7 +202,7 @@ def test_e2g_n384_sampled_grid_points_match_reference(ctx):
     and box-face grid points, against the reference's eval_u_BI_nearSurfc /
     eval_p_BI_nearSurfc (run on an index grid holding only the sample) and its
     plain sums stokes_SL_away / stokes_pressure_away; FP64 to 1e-12, mixed and
-    FP32 to 1e-6."""
+    FP32 to 1e-7."""
     N = 384
     M = N + 1
     e = highreg.E2G(ctx, N)
@@ -234,8 +234,8 @@ def test_e2g_n384_sampled_grid_points_match_reference(ctx):
     fxyz = np.stack(np.unravel_index(face, (M, M, M)), axis=1).astype(np.float64) * (3.0 / N)
     uf_ref, pf_ref = R.away_points(fxyz.ravel())
     print("E2G N=384 sampled sums vs the reference (max / l2):")
-    for prec, name, tol in ((highreg.HR_FP64, "fp64", 1e-12), (highreg.HR_MIXED, "mixed", 1e-6),
-                            (highreg.HR_FP32, "fp32", 1e-6)):
+    for prec, name, tol in ((highreg.HR_FP64, "fp64", 1e-12), (highreg.HR_MIXED, "mixed", 1e-7),
+                            (highreg.HR_FP32, "fp32", 1e-7)):
         e.run(prec)
         p = e.get(0)
         u = e.get(1).reshape(3, -1)

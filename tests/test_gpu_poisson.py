@@ -24,12 +24,27 @@ def test_dst_poisson_round_trip(ctx, oracle):
     assert rel_err(ctx.dst_poisson3d(n, f), oracle.dst_poisson(n, f)) < 1e-12
 
 
-@pytest.mark.parametrize("n", [1, 3, 5, 13, 21, 47, 95, 127, 193])
+@pytest.mark.parametrize("n", [1, 3, 5, 13, 21, 47, 95, 127, 191, 193])
 def test_dst_poisson_line_lengths(ctx, oracle, n):
-    # every FFT stage kind: none (n = 1), radix 2, 3, 4, 8 and direct prime
-    # stages (7, 11, 97), against the oracle's direct O(n^4) transform
+    # every FFT stage kind of the shared-memory pass: none (n = 1), radix 2,
+    # 3, 4, 8 and direct prime stages (7, 11, 97), and the register pass
+    # (n = 64 R - 1: 127 with R = 2, 191 with R = 3), against the oracle's
+    # direct O(n^4) transform
     f = np.random.default_rng(n).standard_normal(n ** 3)
     assert rel_err(ctx.dst_poisson3d(n, f), oracle.dst_poisson(n, f)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [255, 383, 511])
+def test_dst1_register_pass_full_lines(ctx, n):
+    # the register pass at R = 4, 6 (the N = 384 grid), 8: the plain 3D DST-I
+    # against scipy's DST-I (type 1, unnormalised: FFTW's RODFT00) on the
+    # whole cube
+    import scipy.fft as sf
+
+    f = np.random.default_rng(n).standard_normal(n ** 3)
+    got = ctx.dst1_3d(n, f).reshape(n, n, n)
+    ref = sf.dstn(f.reshape(n, n, n), type=1, workers=-1)
+    assert rel_err(got, ref) < 1e-12
 
 
 def test_dst_poisson_full_size_operator(ctx):
