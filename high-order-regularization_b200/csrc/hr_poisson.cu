@@ -331,19 +331,21 @@ __global__ void __launch_bounds__(kDstThreads, 4)
 // Register DST-I pass for lines of n = 64 R - 1 points (N = 64 R, complex
 // length P = 32 R; R = 2, 3, 4, 6, 8: the N = 384 grid is R = 6): one warp
 // per line, the complex sequence held as R values per lane (element
-// m = 32 a + b in register a of lane b), so the FFT runs in registers and
-// warp shuffles and shared memory only stages the rotated store.
+// m = 32 a + bitrev5(b) in register a of lane b), so the FFT runs in
+// registers and warp shuffles and shared memory only stages the rotated store.
 //   1. y_j of the auxiliary-array method, read straight from global memory
-//      (lane b needs x_{j}, x_{j+1} and their mirrors for j = 64 a + 2 b);
+//      (lane b needs x_j, x_{j+1} and their mirrors for j = 64 a + 2 m_b; a
+//      warp's reads cover 64 consecutive points per a, in a permuted order);
 //   2. P = R x 32: an R-point DFT over each lane's registers, the twiddles
-//      W_P^{b k1}, then a 32-point decimation-in-frequency DFT across the
-//      lanes (five butterfly stages with shuffles), leaving Z_{k1 + R k2} in
-//      register k1 of lane bitrev5(k2);
+//      W_P^{m_b k1}, then a 32-point decimation-in-time DFT across the lanes
+//      (five butterfly stages with shuffles; bit-reversed input, natural
+//      output), leaving Z_{k1 + R b} in register k1 of lane b;
 //   3. the real split with the partner Z_{P-k} fetched by one shuffle per
 //      register (lane b ^ 31 for k1 > 0), and the odd-output recurrence as an
-//      in-lane prefix over k1 plus a warp scan over k2;
-//   4. the CTA's kDstLines lines written rotated through shared memory with
-//      the pass's epilogue, as in dst_pass_kernel.
+//      in-lane prefix over k1 plus a warp scan over the lanes;
+//   4. the CTA's kDstLines lines written rotated through shared memory (even
+//      and odd outputs in separate regions: lanes' stores two-way at most)
+//      with the pass's epilogue, as in dst_pass_kernel.
 
 __device__ __forceinline__ void dft6(double2* v) {
   // 6 = 2 x 3: DFTs of the even and the odd elements, then W6^k
@@ -361,14 +363,13 @@ __device__ __forceinline__ void dft6(double2* v) {
   v[5] = csub(e2, t2);
 }
 
+// Forward R-point DFT of registers, natural order in and out.
 template <int R>
 __device__ __forceinline__ void dft_regs(double2* v) {
   if constexpr (R == 2) dft2(v[0], v[1]);
   else if constexpr (R == 3) dft3(v[0], v[1], v[2]);
-  else if constexpr (R == 4) {
-    dft4(v[0], v[1], v[2], v[3]);
-    // dft4 leaves outputs in order 0, 1, 2, 3 (a0, a1, a2, a3)
-  } else if constexpr (R == 6) dft6(v);
+  else if constexpr (R == 4) dft4(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 6) dft6(v);
   else dft8(v);
 }
 
@@ -394,14 +395,15 @@ __global__ void __launch_bounds__(kDstThreads, 3)
   const int nt = (int)min((long)T, lines - l0);
   const int t = threadIdx.x >> 5, b = threadIdx.x & 31;
   const bool live = t < nt;
+  const int mb = brev5(b);
 
-  // 1. z_m = y_{2m} + i y_{2m+1}, m = 32 a + b
+  // 1. z_m = y_{2m} + i y_{2m+1}, m = 32 a + bitrev5(b)
   double2 z[R];
   {
     const double* row = in + (l0 + (live ? t : 0)) * n;
 #pragma unroll
     for (int a = 0; a < R; a++) {
-      const int j = 64 * a + 2 * b;
+      const int j = 64 * a + 2 * mb;
       double yr = 0.0, yi = 0.0;
       if (live) {
         if (j > 0) {
@@ -415,37 +417,39 @@ __global__ void __launch_bounds__(kDstThreads, 3)
     }
   }
 
-  // 2. Z_{k1 + R k2} = sum_b W32^{b k2} W_P^{b k1} sum_a z_{32 a + b} W_R^{a k1}
+  // 2. Z_{k1 + R k2} = sum_m2 W32^{m2 k2} W_P^{m2 k1} sum_a z_{32 a + m2} W_R^{a k1}
   dft_regs<R>(z);
 #pragma unroll
-  for (int k1 = 1; k1 < R; k1++) z[k1] = cmul(z[k1], __ldg(&tw[2 * b * k1]));  // W_P^x = tw[2x]
+  for (int k1 = 1; k1 < R; k1++) z[k1] = cmul(z[k1], __ldg(&tw[2 * mb * k1]));  // W_P^x = tw[2x]
 #pragma unroll
-  for (int s = 16; s >= 1; s >>= 1) {
+  for (int s = 1; s <= 16; s <<= 1) {
+    // radix-2 DIT across lanes: pair (L, L + s) with a = x_L, c = x_{L+s},
+    // omega = W_{2s}^{L mod s}: x_L = a + omega c, x_{L+s} = a - omega c
     const bool upper = (b & s) != 0;
     const double sg = upper ? -1.0 : 1.0;
-    // W_{2s}^{i}, i = b mod s, for the upper lanes; 1 for the lower ones
-    const double2 wt = (s > 1 && upper) ? __ldg(&tw[(b & (s - 1)) * (N / (2 * s))]) : make_double2(1.0, 0.0);
+    const double2 om = s > 1 ? __ldg(&tw[(b & (s - 1)) * (N / (2 * s))]) : make_double2(1.0, 0.0);
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++) {
       const double2 p = make_double2(__shfl_xor_sync(0xffffffffu, z[k1].x, s),
                                      __shfl_xor_sync(0xffffffffu, z[k1].y, s));
-      const double2 q = make_double2(fma(sg, z[k1].x, p.x), fma(sg, z[k1].y, p.y));  // lower: p + z; upper: p - z
-      z[k1] = s > 1 ? cmul(q, wt) : q;
+      const double2 c = upper ? z[k1] : p;   // the upper element
+      const double2 a0 = upper ? p : z[k1];  // the lower element
+      const double2 oc = s > 1 ? cmul(c, om) : c;
+      z[k1] = make_double2(fma(sg, oc.x, a0.x), fma(sg, oc.y, a0.y));
     }
   }
-  // lane b now holds Z_k, k = k1 + R k2 with k2 = bitrev5(b)
-  const int k2 = brev5(b);
+  // lane b now holds Z_k, k = k1 + R b
 
   // 3. real split: partner Z_{P - k}: k1 > 0 -> register R - k1 of lane b ^ 31;
-  //    k1 = 0 -> register 0 of lane bitrev5((32 - k2) mod 32)
+  //    k1 = 0 -> register 0 of lane (32 - b) mod 32
   double ev[R], od[R];
   {
-    const int src0 = brev5((32 - k2) & 31);
+    const int src0 = (32 - b) & 31;
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++) {
       const double2 a = z[k1];
       const double2 c = k1 == 0 ? shfl2(z[0], src0) : shfl2(z[R - k1], b ^ 31);
-      const int k = k1 + R * k2;
+      const int k = k1 + R * b;
       if (k == 0) {
         ev[k1] = a.x + a.y;  // R_0
         od[k1] = 0.0;
@@ -455,32 +459,33 @@ __global__ void __launch_bounds__(kDstThreads, 3)
         const double2 wk = __ldg(&tw[k]);
         const double Yx = Ex + (wk.x * Ox - wk.y * Oy);
         const double Yy = Ey + (wk.x * Oy + wk.y * Ox);
-        ev[k1] = 2.0 * Yx;  // summed into the even outputs below
-        od[k1] = -2.0 * Yy; // output 2k - 1
+        ev[k1] = 2.0 * Yx;   // summed into the even outputs below
+        od[k1] = -2.0 * Yy;  // output 2k - 1
       }
     }
   }
-  // even outputs: 2F at 2k = R_0 + sum_{k' = 1..k} 2 Yx_{k'} (natural order k = k1 + R k2)
+  // even outputs: 2F at 2k = R_0 + sum_{k' = 1..k} 2 Yx_{k'} (natural order k = k1 + R b)
   {
 #pragma unroll
     for (int k1 = 1; k1 < R; k1++) ev[k1] += ev[k1 - 1];
     double incl = ev[R - 1];
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-      const double x = __shfl_sync(0xffffffffu, incl, brev5((k2 - d) & 31));
-      if (k2 >= d) incl += x;
+      const double x = __shfl_up_sync(0xffffffffu, incl, d);
+      if (b >= d) incl += x;
     }
     const double excl = incl - ev[R - 1];
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++) ev[k1] += excl;
   }
-  // stage this line's outputs for the rotated store: output 2k (even), 2k - 1 (odd)
-  double* tile = dsm;
+  // stage the outputs: even 2k at E[k], odd 2k - 1 at O[k - 1] (columns: lines)
+  double* E = dsm;
+  double* O = dsm + P * RS;
 #pragma unroll
   for (int k1 = 0; k1 < R; k1++) {
-    const int k = k1 + R * k2;
-    tile[(2 * k) * RS + t] = ev[k1];
-    if (k > 0) tile[(2 * k - 1) * RS + t] = od[k1];
+    const int k = k1 + R * b;
+    E[k * RS + t] = ev[k1];
+    if (k > 0) O[(k - 1) * RS + t] = od[k1];
   }
   __syncthreads();
 
@@ -489,7 +494,7 @@ __global__ void __launch_bounds__(kDstThreads, 3)
     const int kk = idx / T, tt = idx - kk * T;
     if (tt >= nt) continue;
     const long l = l0 + tt;
-    const double F2 = tile[kk * RS + tt];
+    const double F2 = (kk & 1) ? O[(kk >> 1) * RS + tt] : E[(kk >> 1) * RS + tt];
     if (mode == 0) {
       out[kk * lines + l] = F2;
     } else if (mode == 3) {
@@ -671,7 +676,7 @@ struct DstPlan {
     if (R == 2 || R == 3 || R == 4 || R == 6 || R == 8) {
       fn = R == 2 ? dst_pass_reg_kernel<2> : R == 3 ? dst_pass_reg_kernel<3> : R == 4 ? dst_pass_reg_kernel<4>
          : R == 6 ? dst_pass_reg_kernel<6> : dst_pass_reg_kernel<8>;
-      smem = (size_t)n * (kDstLines + 1) * sizeof(double);
+      smem = (size_t)(n + 1) * (kDstLines + 1) * sizeof(double);  // P rows of even, P of odd outputs
     } else {
       fn = P == 48 ? dst_pass_kernel<48> : P == 24 ? dst_pass_kernel<24> : dst_pass_kernel<0>;
       smem = 2 * (size_t)dst_bufd(P) * sizeof(double);
