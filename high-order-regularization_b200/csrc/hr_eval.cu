@@ -627,12 +627,20 @@ __device__ __forceinline__ void proxies64_rows(const double2* __restrict__ s2, i
   }
 }
 
-// FP32 proxies, FP64 accumulation per Chebyshev row.
-template <bool DL>
-__device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, int row0, int nrows, int P1,
+// FP32 proxies, FP64 accumulation per Chebyshev row. P1C > 0 compiles the
+// row length (the proxy loop unrolls and the z coordinates stay in
+// registers); P1C = 0 takes any P1.
+template <bool DL, int P1C>
+__device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, int row0, int nrows, int P1rt,
                                                const float* __restrict__ chebf, const Tgt32& F, double& a0,
                                                double& a1, double& a2) {
   constexpr int W = DL ? 3 : 2;  // float4 per proxy
+  const int P1 = P1C > 0 ? P1C : P1rt;
+  float dz[P1C > 0 ? P1C : 1];
+  if constexpr (P1C > 0) {
+#pragma unroll
+    for (int pk = 0; pk < P1C; pk++) dz[pk] = F.pz - chebf[2 * P1C + pk];
+  }
   for (int r = 0; r < nrows; r++) {
     const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
     const float d0 = F.px - chebf[pi];
@@ -642,8 +650,9 @@ __device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, in
     const float g0r = F.g0[0] * d0 + F.g0[1] * d1;
     const float4* row = s4 + r * P1 * W;
     float p0 = 0.f, p1 = 0.f, p2 = 0.f;
-    for (int pk = 0; pk < P1; pk++) {
-      const float d2 = F.pz - chebf[2 * P1 + pk];
+#pragma unroll
+    for (int pk = 0; pk < (P1C > 0 ? P1C : P1); pk++) {
+      const float d2 = P1C > 0 ? dz[pk] : F.pz - chebf[2 * P1 + pk];
       const float rinv = rsqrtf(fmaf(d2, d2, r01));
       const float4 A = row[pk * W];
       const float4 B = row[pk * W + 1];
@@ -670,6 +679,18 @@ __device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, in
     a0 += (double)p0;
     a1 += (double)p1;
     a2 += (double)p2;
+  }
+}
+
+template <bool DL>
+__device__ __forceinline__ void proxies32_any(const float4* __restrict__ s4, int row0, int nrows, int P1,
+                                              const float* __restrict__ chebf, const Tgt32& F, double& a0,
+                                              double& a1, double& a2) {
+  switch (P1) {  // the treecode degrees in use: P = 5 (inner), 6 (h = 1/64), 10 (h = 1/256)
+    case 6: proxies32_rows<DL, 6>(s4, row0, nrows, P1, chebf, F, a0, a1, a2); break;
+    case 7: proxies32_rows<DL, 7>(s4, row0, nrows, P1, chebf, F, a0, a1, a2); break;
+    case 11: proxies32_rows<DL, 11>(s4, row0, nrows, P1, chebf, F, a0, a1, a2); break;
+    default: proxies32_rows<DL, 0>(s4, row0, nrows, P1, chebf, F, a0, a1, a2);
   }
 }
 
@@ -852,7 +873,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
         if (act) {
           const char* cur = buf + (ch & 1) * kHalf;
           if (MIXED)
-            proxies32_rows<DL>(reinterpret_cast<const float4*>(cur), row0, rows, P1, wchebf, F, a0, a1, a2);
+            proxies32_any<DL>(reinterpret_cast<const float4*>(cur), row0, rows, P1, wchebf, F, a0, a1, a2);
           else
             proxies64_rows<DL>(reinterpret_cast<const double2*>(cur), row0, rows, P1, wcheb, S, a0, a1, a2);
         }
@@ -886,12 +907,19 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
 // ------------------------------------- two targets per thread (mixed, on-surface)
 
 // FP32 proxies of a run of Chebyshev rows for two targets: each shared-memory
-// read of a proxy serves both. Sums per row go to acc (FP64).
-template <bool DL>
-__device__ __forceinline__ void proxies32_rows2(const float4* __restrict__ s4, int row0, int nrows, int P1,
+// read of a proxy serves both. Sums per row go to acc (FP64). P1C as in
+// proxies32_rows.
+template <bool DL, int P1C>
+__device__ __forceinline__ void proxies32_rows2(const float4* __restrict__ s4, int row0, int nrows, int P1rt,
                                                 const float* __restrict__ chebf, const Tgt32 (&F)[2],
                                                 double (&acc)[2][3]) {
   constexpr int W = DL ? 3 : 2;  // float4 per proxy
+  const int P1 = P1C > 0 ? P1C : P1rt;
+  float czr[P1C > 0 ? P1C : 1];
+  if constexpr (P1C > 0) {
+#pragma unroll
+    for (int pk = 0; pk < P1C; pk++) czr[pk] = chebf[2 * P1C + pk];
+  }
   for (int r = 0; r < nrows; r++) {
     const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
     const float cx = chebf[pi], cy = chebf[P1 + pj];
@@ -908,8 +936,9 @@ __device__ __forceinline__ void proxies32_rows2(const float4* __restrict__ s4, i
       g0r[q] = F[q].g0[0] * d0[q] + F[q].g0[1] * d1[q];
     }
     const float4* row = s4 + r * P1 * W;
-    for (int pk = 0; pk < P1; pk++) {
-      const float cz = chebf[2 * P1 + pk];
+#pragma unroll
+    for (int pk = 0; pk < (P1C > 0 ? P1C : P1); pk++) {
+      const float cz = P1C > 0 ? czr[pk] : chebf[2 * P1 + pk];
       const float4 A = row[pk * W];
       const float4 B = row[pk * W + 1];
       const float Cx = DL ? reinterpret_cast<const float*>(row + pk * W + 2)[0] : 0.f;
@@ -941,6 +970,18 @@ __device__ __forceinline__ void proxies32_rows2(const float4* __restrict__ s4, i
 #pragma unroll
     for (int q = 0; q < 2; q++)
       for (int c = 0; c < 3; c++) acc[q][c] += (double)p[q][c];
+  }
+}
+
+template <bool DL>
+__device__ __forceinline__ void proxies32_any2(const float4* __restrict__ s4, int row0, int nrows, int P1,
+                                               const float* __restrict__ chebf, const Tgt32 (&F)[2],
+                                               double (&acc)[2][3]) {
+  switch (P1) {  // the treecode degrees in use: P = 5 (inner), 6 (h = 1/64), 10 (h = 1/256)
+    case 6: proxies32_rows2<DL, 6>(s4, row0, nrows, P1, chebf, F, acc); break;
+    case 7: proxies32_rows2<DL, 7>(s4, row0, nrows, P1, chebf, F, acc); break;
+    case 11: proxies32_rows2<DL, 11>(s4, row0, nrows, P1, chebf, F, acc); break;
+    default: proxies32_rows2<DL, 0>(s4, row0, nrows, P1, chebf, F, acc);
   }
 }
 
@@ -1051,7 +1092,7 @@ __device__ __forceinline__ void run_item_on2(const EvalTask& T, const BlockRef& 
         }
         __syncwarp();
         if (actA || actB)
-          proxies32_rows2<DL>(reinterpret_cast<const float4*>(buf + (ch & 1) * kHalf), row0, rows, P1, wchebf, F,
+          proxies32_any2<DL>(reinterpret_cast<const float4*>(buf + (ch & 1) * kHalf), row0, rows, P1, wchebf, F,
                               acc);
         __syncwarp();
       }
@@ -1104,10 +1145,14 @@ __global__ void __launch_bounds__(kTB2, 8) eval_kernel_on2(const EvalTask* __res
 // ON = true: the batch's lean items only — on-surface kinds (K_SL_ON / K_DL_ON)
 // or, for the extend-to-grid family, the plain box-face sums (K_E2G_*_AWAY).
 // Their code path needs fewer registers than the others' (no nearest-point
-// data, no per-target regularization coefficients), so it runs with five
-// (box-face sums: six) resident CTAs per SM instead of four.
+// data, no per-target regularization coefficients), so it runs with more
+// resident CTAs per SM: six (80 registers) for the Stokeslet and box-face
+// sums, five (96) for the stresslet, whose larger smoothing table fills the
+// shared memory of a sixth (its degree-11 table that would fit measured
+// slower). The FP64 off-surface Stokeslet items fit 96 registers without
+// spills and run five CTAs per SM; the other off-surface kernels four.
 template <int FAM, bool MIXED, bool ON, bool COUNT>
-__global__ void __launch_bounds__(kTB, ON ? (FAM == F_E2G ? 6 : 5) : 4)
+__global__ void __launch_bounds__(kTB, ON ? (FAM == F_DL ? 5 : 6) : ((FAM == F_SL && !MIXED) ? 5 : 4))
     eval_kernel(const EvalTask* __restrict__ tasks, const BlockRef* __restrict__ items,
                 const Seg* __restrict__ segs) {
   __shared__ __align__(16) double sm[kSmem];
