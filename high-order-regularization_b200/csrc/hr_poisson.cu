@@ -332,11 +332,10 @@ __global__ void __launch_bounds__(kDstThreads, 4)
 // length P = 32 R; R = 2, 3, 4, 6, 8: the N = 384 grid is R = 6): one warp
 // per line, the complex sequence held as R values per lane (element
 // m = 32 a + bitrev5(b) in register a of lane b), so the FFT runs in
-// registers and warp shuffles; shared memory stages the line and the rotated
-// store.
-//   1. y_j of the auxiliary-array method from the line, read coalesced into
-//      shared memory (lane b needs x_j, x_{j+1} and their mirrors for
-//      j = 64 a + 2 m_b);
+// registers and warp shuffles and shared memory only stages the rotated store.
+//   1. y_j of the auxiliary-array method, read straight from global memory
+//      (lane b needs x_j, x_{j+1} and their mirrors for j = 64 a + 2 m_b; a
+//      warp's reads cover 64 consecutive points per a, in a permuted order);
 //   2. P = R x 32: an R-point DFT over each lane's registers, the twiddles
 //      W_P^{m_b k1}, then a 32-point decimation-in-time DFT across the lanes
 //      (five butterfly stages with shuffles; bit-reversed input, natural
@@ -398,41 +397,25 @@ __global__ void __launch_bounds__(kDstThreads, 3)
   const bool live = t < nt;
   const int mb = brev5(b);
 
-  // 1. the line, read coalesced (lane b takes points b + 32 c) into this
-  // warp's slot of shared memory one place up (point e at e + 1, so the
-  // pairs (x_{j-1}, x_j) of even j are aligned double2s), then
-  // z_m = y_{2m} + i y_{2m+1}, m = 32 a + bitrev5(b)
+  // 1. z_m = y_{2m} + i y_{2m+1}, m = 32 a + bitrev5(b)
   double2 z[R];
   {
-    double* buf = dsm + t * N;  // N doubles per warp (point e at e + 1; slot 0 unused)
-    if (live) {
-      const double* row = in + (l0 + t) * n;
-#pragma unroll
-      for (int c = 0; c < (n + 31) / 32; c++) {
-        const int e = b + 32 * c;
-        if (e < n) buf[e + 1] = row[e];
-      }
-    }
-    __syncwarp();
+    const double* row = in + (l0 + (live ? t : 0)) * n;
 #pragma unroll
     for (int a = 0; a < R; a++) {
       const int j = 64 * a + 2 * mb;
       double yr = 0.0, yi = 0.0;
       if (live) {
-        const double2 xp = *reinterpret_cast<const double2*>(buf + j);  // (x_{j-1}, x_j) as row[j - 1], row[j]
-        const double xm1 = buf[N - j - 1];                                // row[N - j - 2]
         if (j > 0) {
-          const double xm = buf[N - j];  // row[N - j - 1]
-          yr = __ldg(&sintab[j]) * (xp.x + xm) + 0.5 * (xp.x - xm);
+          const double xj = row[j - 1], xm = row[N - j - 1];
+          yr = __ldg(&sintab[j]) * (xj + xm) + 0.5 * (xj - xm);
         }
-        yi = __ldg(&sintab[j + 1]) * (xp.y + xm1) + 0.5 * (xp.y - xm1);
+        const double xj1 = row[j], xm1 = row[N - j - 2];
+        yi = __ldg(&sintab[j + 1]) * (xj1 + xm1) + 0.5 * (xj1 - xm1);
       }
       z[a] = make_double2(yr, yi);
     }
   }
-  // every warp has read its line before the output tile (the same shared
-  // memory) is written
-  __syncthreads();
 
   // 2. Z_{k1 + R k2} = sum_m2 W32^{m2 k2} W_P^{m2 k1} sum_a z_{32 a + m2} W_R^{a k1}
   dft_regs<R>(z);
@@ -604,59 +587,33 @@ __global__ void __launch_bounds__(128) extend_kernel(int N, double L, double h, 
 
 // 4th-order compact Laplacian RHS (lapl_4ord_inCube, lapl_4ord_nearSurfc,
 // dp_d{x,y,z}_4ord: E2G/main.cpp:1566-1823), one fused pass over the interior.
-// One CTA per interior plane i and kRhsRows consecutive rows j: the 3 x
-// (kRhsRows + 2) rows of w its 15-point stencils read are staged in shared
-// memory once (coalesced along k), so each row of w is read from L2 about
-// 3 (kRhsRows + 2) / kRhsRows times instead of nine; u (BAND2 points only)
-// and p (the pressure-gradient term) are read from global memory.
-constexpr int kRhsRows = 4;
-constexpr int kRhsThreads = 256;
-__global__ void __launch_bounds__(kRhsThreads)
+// One CTA per interior row (i, j), threads along k, each of the nine
+// neighbouring rows of w and u addressed from its own row pointer.
+__global__ void __launch_bounds__(128)
     rhs_kernel(int N, double h, const double* __restrict__ Gw, const double* __restrict__ u,
                const uint8_t* __restrict__ band2, const uint8_t* __restrict__ outside,
                const double* __restrict__ p, int axis, double* __restrict__ rhs) {
-  extern __shared__ __align__(16) double wsm[];  // [3][kRhsRows + 2][M]
   const long M = N + 1;
   const long n = N - 1;
-  const int i = blockIdx.y + 1;
-  const int j0 = blockIdx.x * kRhsRows + 1;
-  const int nj = min(kRhsRows, N - j0);  // rows j0 .. j0 + nj - 1 (j <= N - 1)
-  const long si = M * M, sj = M;
-  constexpr int SR = kRhsRows + 2;
-  // stage w rows (i + di, j0 - 1 + r, all k), di = -1..1, r = 0..nj + 1
-  for (int q = threadIdx.x; q < 3 * SR * (int)M; q += kRhsThreads) {
-    const int pl = q / (SR * (int)M), rem = q - pl * SR * (int)M;
-    const int r = rem / (int)M, k = rem - r * (int)M;
-    if (r <= nj + 1) wsm[q] = Gw[(long)(i - 1 + pl) * si + (long)(j0 - 1 + r) * sj + k];
-  }
-  __syncthreads();
-  auto W = [&](int di, int r, int k) { return wsm[((di + 1) * SR + r) * M + k]; };
+  const int j = blockIdx.x + 1, i = blockIdx.y + 1;
+  const long c0 = ((long)i * M + j) * M;  // row (i, j)
+  const long sj = M, si = M * M;
   const long gst = axis == 0 ? si : (axis == 1 ? sj : 1);
-  for (int q = threadIdx.x; q < nj * (int)(n); q += kRhsThreads) {
-    const int jj = q / (int)n;
-    const int k = q - jj * (int)n + 1;
-    const int j = j0 + jj;
-    const int r = jj + 1;  // staged row of j
-    const long c0 = ((long)i * M + j) * M;
-    // -(2/3) Lap_h w from the staged rows (lapl_4ord_inCube, E2G/main.cpp:1566-1609)
-    const double ctr = W(0, r, k);
-    double lap7 = W(1, r, k) + W(-1, r, k) + W(0, r + 1, k) + W(0, r - 1, k) + W(0, r, k + 1) + W(0, r, k - 1) -
-                  6.0 * ctr;
-    double temp1 = W(1, r + 1, k + 1) + W(1, r - 1, k + 1) + W(-1, r + 1, k + 1) + W(-1, r - 1, k + 1) - 4.0 * ctr;
-    double temp2 = W(1, r + 1, k - 1) + W(1, r - 1, k - 1) + W(-1, r + 1, k - 1) + W(-1, r - 1, k - 1) - 4.0 * ctr;
-    double res = -2.0 / 3.0 * (lap7 + (temp1 + temp2) / 8.0);
-    if (band2[c0 + k]) {
-      // +(2/3) Lap_h u at BAND2 points (lapl_4ord_nearSurfc, E2G/main.cpp:1611-1652)
-      const double* r0 = u + c0 + k;
-      const double uc = r0[0];
-      double l7 = r0[si] + r0[-si] + r0[sj] + r0[-sj] + r0[1] + r0[-1] - 6.0 * uc;
-      double t1 = r0[si + sj + 1] + r0[si - sj + 1] + r0[-si + sj + 1] + r0[-si - sj + 1] - 4.0 * uc;
-      double t2 = r0[si + sj - 1] + r0[si - sj - 1] + r0[-si + sj - 1] + r0[-si - sj - 1] - 4.0 * uc;
-      res += 2.0 / 3.0 * (l7 + (t1 + t2) / 8.0);
-    }
+  const int c = axis == 0 ? i : (axis == 1 ? j : 0);
+  double* out = rhs + ((long)(i - 1) * n + (j - 1)) * n;  // out[k - 1] = rhs(i, j, k)
+  auto lap = [&](const double* a, int k) {
+    const double* r0 = a + c0 + k;
+    const double ctr = r0[0];
+    double lap7 = r0[si] + r0[-si] + r0[sj] + r0[-sj] + r0[1] + r0[-1] - 6.0 * ctr;
+    double temp1 = r0[si + sj + 1] + r0[si - sj + 1] + r0[-si + sj + 1] + r0[-si - sj + 1] - 4.0 * ctr;
+    double temp2 = r0[si + sj - 1] + r0[si - sj - 1] + r0[-si + sj - 1] + r0[-si - sj - 1] - 4.0 * ctr;
+    return lap7 + (temp1 + temp2) / 8.0;
+  };
+  for (int k = threadIdx.x + 1; k < N; k += blockDim.x) {
+    double r = -2.0 / 3.0 * lap(Gw, k);
+    if (band2[c0 + k]) r += 2.0 / 3.0 * lap(u, k);
     if (axis >= 0 && outside[c0 + k]) {
-      // + h dp/dx_axis outside BAND2 (dp_d{x,y,z}_4ord, E2G/main.cpp:1654-1823)
-      const int cc = axis == 0 ? i : (axis == 1 ? j : k);
+      const int cc = axis == 2 ? k : c;
       const double* pc = p + c0 + k;
       auto P = [&](int o) { return pc[o * gst]; };
       double d;
@@ -668,9 +625,9 @@ __global__ void __launch_bounds__(kRhsThreads)
         d = -P(2) + 8.0 * P(1) - 8.0 * P(-1) + P(-2);
         d /= 12.0;
       }
-      res += d * h;
+      r += d * h;
     }
-    rhs[((long)(i - 1) * n + (j - 1)) * n + (k - 1)] = res;
+    out[k - 1] = r;
   }
 }
 
@@ -719,8 +676,7 @@ struct DstPlan {
     if (R == 2 || R == 3 || R == 4 || R == 6 || R == 8) {
       fn = R == 2 ? dst_pass_reg_kernel<2> : R == 3 ? dst_pass_reg_kernel<3> : R == 4 ? dst_pass_reg_kernel<4>
          : R == 6 ? dst_pass_reg_kernel<6> : dst_pass_reg_kernel<8>;
-      // P rows of even and P of odd outputs; it also holds the kDstLines staged input lines
-      smem = (size_t)(n + 1) * (kDstLines + 1) * sizeof(double);
+      smem = (size_t)(n + 1) * (kDstLines + 1) * sizeof(double);  // P rows of even, P of odd outputs
     } else {
       fn = P == 48 ? dst_pass_kernel<48> : P == 24 ? dst_pass_kernel<24> : dst_pass_kernel<0>;
       smem = 2 * (size_t)dst_bufd(P) * sizeof(double);
@@ -847,12 +803,7 @@ void solve_poisson_dev(Ctx& C, int N, double L, const uint8_t* band2_dev, const 
   DBuf<double>& rhs = work->rhs;
   extend_kernel<<<dim3(M, (M + kExtRows - 1) / kExtRows), 128, 0, C.stream>>>(N, L, h, u_dev, w.p);
   const int axis = (variable >= 1 && variable <= 3) ? variable - 1 : -1;
-  {
-    const size_t rsm = (size_t)3 * (kRhsRows + 2) * M * sizeof(double);
-    HR_CHECK_CUDA(cudaFuncSetAttribute(rhs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsm));
-    rhs_kernel<<<dim3((n + kRhsRows - 1) / kRhsRows, n), kRhsThreads, rsm, C.stream>>>(N, h, w.p, u_dev, band2_dev,
-                                                                                     out_dev, p_dev, axis, rhs.p);
-  }
+  rhs_kernel<<<dim3(n, n), 128, 0, C.stream>>>(N, h, w.p, u_dev, band2_dev, out_dev, p_dev, axis, rhs.p);
   // u = w on the boundary; the interior gets w + the scaled solution
   faces_copy_kernel<<<dim3(M, 6), 128, 0, C.stream>>>(M, w.p, u_dev);
   C.launches += 3;
