@@ -585,11 +585,12 @@ __device__ __forceinline__ void copy_async_wait() {
 // the reference's proxy sum (Call_Treecode_DL, 2S/KITC.cpp:753-771)
 // regrouped, with d.M.d from the symmetric part and the products of d0, d1
 // taken once per row; Call_Treecode_SL (2S/KITC.cpp:700-714) as written.
-template <bool DL>
-__device__ __forceinline__ void proxies64_rows(const double2* __restrict__ s2, int row0, int nrows, int P1,
+template <bool DL, int P1C>
+__device__ __forceinline__ void proxies64_rows(const double2* __restrict__ s2, int row0, int nrows, int P1rt,
                                                const double* __restrict__ cheb, const Tgt& S, double& a0,
                                                double& a1, double& a2) {
   constexpr int W = DL ? 5 : 3;  // double2 per proxy
+  const int P1 = P1C > 0 ? P1C : P1rt;
   for (int r = 0; r < nrows; r++) {
     const int pi = (row0 + r) / P1, pj = (row0 + r) - pi * P1;
     const double d0 = S.px - cheb[pi];
@@ -598,7 +599,8 @@ __device__ __forceinline__ void proxies64_rows(const double2* __restrict__ s2, i
     const double d00 = d0 * d0, d11 = d1 * d1, d01 = d0 * d1;
     const double g0r = S.g0[0] * d0 + S.g0[1] * d1;
     const double2* row = s2 + r * P1 * W;
-    for (int pk = 0; pk < P1; pk++) {
+#pragma unroll
+    for (int pk = 0; pk < (P1C > 0 ? P1C : P1); pk++) {
       const double d2 = S.pz - cheb[2 * P1 + pk];
       const double rinv = rsqrt(fma(d2, d2, r01));
       const double2* m = row + pk * W;
@@ -679,6 +681,17 @@ __device__ __forceinline__ void proxies32_rows(const float4* __restrict__ s4, in
     a0 += (double)p0;
     a1 += (double)p1;
     a2 += (double)p2;
+  }
+}
+
+template <bool DL>
+__device__ __forceinline__ void proxies64_any(const double2* __restrict__ s2, int row0, int nrows, int P1,
+                                              const double* __restrict__ cheb, const Tgt& S, double& a0, double& a1,
+                                              double& a2) {
+  switch (P1) {  // the treecode degrees in use: P = 6 (h = 1/64), 10 (h = 1/256)
+    case 7: proxies64_rows<DL, 7>(s2, row0, nrows, P1, cheb, S, a0, a1, a2); break;
+    case 11: proxies64_rows<DL, 11>(s2, row0, nrows, P1, cheb, S, a0, a1, a2); break;
+    default: proxies64_rows<DL, 0>(s2, row0, nrows, P1, cheb, S, a0, a1, a2);
   }
 }
 
@@ -875,7 +888,7 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           if (MIXED)
             proxies32_any<DL>(reinterpret_cast<const float4*>(cur), row0, rows, P1, wchebf, F, a0, a1, a2);
           else
-            proxies64_rows<DL>(reinterpret_cast<const double2*>(cur), row0, rows, P1, wcheb, S, a0, a1, a2);
+            proxies64_any<DL>(reinterpret_cast<const double2*>(cur), row0, rows, P1, wcheb, S, a0, a1, a2);
         }
         __syncwarp();
       }
