@@ -838,8 +838,13 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           }
         } else {
           unsigned cr = 0;
+          if (cnt == kNT) {  // a full tile: a compile-time trip count
+#pragma unroll 4
+            for (int j = 0; j < kNT; j++) cr += pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
+          } else {
 #pragma unroll 2
-          for (int j = 0; j < cnt; j++) cr += pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
+            for (int j = 0; j < cnt; j++) cr += pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
+          }
           if (kCount) {
             if (S.near) {
               creg += cr;
