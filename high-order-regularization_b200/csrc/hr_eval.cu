@@ -817,7 +817,12 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           for (int j0 = 0; j0 < cnt; j0 += 16) {
             float p0 = 0.f, p1 = 0.f, p2 = 0.f;
             const int j1 = min(cnt, j0 + 16);
-            for (int j = j0; j < j1; j++) pair32<KIND>(ws4, j, F, p0, p1, p2);
+            if (j1 - j0 == 16) {  // a full run: a compile-time trip count
+#pragma unroll 4
+              for (int j = j0; j < j0 + 16; j++) pair32<KIND>(ws4, j, F, p0, p1, p2);
+            } else {
+              for (int j = j0; j < j1; j++) pair32<KIND>(ws4, j, F, p0, p1, p2);
+            }
             a0 += (double)p0;
             a1 += (double)p1;
             a2 += (double)p2;
@@ -1070,11 +1075,20 @@ __device__ __forceinline__ void run_item_on2(const EvalTask& T, const BlockRef& 
         for (int j0 = 0; j0 < cnt; j0 += 16) {
           float pA[3] = {0.f, 0.f, 0.f}, pB[3] = {0.f, 0.f, 0.f};
           const int j1 = min(cnt, j0 + 16);
+          if (j1 - j0 == 16) {  // a full run: a compile-time trip count
+#pragma unroll 4
+            for (int j = j0; j < j0 + 16; j++) {
+              const float4 P = ws4[j], N = ws4[kNT + j], Q = ws4[2 * kNT + j];
+              pair32tab_src<KIND>(P, N, Q, F[0], gf, stab32, pA[0], pA[1], pA[2]);
+              pair32tab_src<KIND>(P, N, Q, F[1], gf, stab32, pB[0], pB[1], pB[2]);
+            }
+          } else {
 #pragma unroll 2
-          for (int j = j0; j < j1; j++) {
-            const float4 P = ws4[j], N = ws4[kNT + j], Q = ws4[2 * kNT + j];
-            pair32tab_src<KIND>(P, N, Q, F[0], gf, stab32, pA[0], pA[1], pA[2]);
-            pair32tab_src<KIND>(P, N, Q, F[1], gf, stab32, pB[0], pB[1], pB[2]);
+            for (int j = j0; j < j1; j++) {
+              const float4 P = ws4[j], N = ws4[kNT + j], Q = ws4[2 * kNT + j];
+              pair32tab_src<KIND>(P, N, Q, F[0], gf, stab32, pA[0], pA[1], pA[2]);
+              pair32tab_src<KIND>(P, N, Q, F[1], gf, stab32, pB[0], pB[1], pB[2]);
+            }
           }
           if (actA)
             for (int c = 0; c < 3; c++) a[0][c] += (double)pA[c];
