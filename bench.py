@@ -128,8 +128,23 @@ def pairs_of(work):
     return work["direct_pairs_near"] + work["direct_pairs_far"] + work["proxy_pairs"]
 
 
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo; None where unreadable)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_reference_matvec(geo_pairs, seconds_budget=None):
-    """One reference operator application on the host cores (oracle/_ref)."""
+    """One reference operator application on the host cores (oracle/_ref),
+    and, for a kernel-for-kernel figure, the reference's four stresslet
+    treecode sums of that operator alone (eval_Stokes_DL_{on,off}Surf_tree,
+    without its serial density-interpolation search): returns (R, seconds of
+    the operator, seconds of the four sums)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import numpy as np
     from oracle import Ref2S
@@ -139,7 +154,12 @@ def cpu_reference_matvec(geo_pairs, seconds_budget=None):
     t0 = time.perf_counter()
     R.matvec(u)
     dt = time.perf_counter() - t0
-    return R, dt
+    # the matvec left the density and its nearest-point interpolation in the scene
+    t0 = time.perf_counter()
+    for s, t in ((0, 0), (0, 1), (1, 0), (1, 1)):
+        R.eval(1, True, s, t)
+    dt_sums = time.perf_counter() - t0
+    return R, dt, dt_sums
 
 
 def run_reference(args, rank, world):
@@ -192,7 +212,7 @@ def run_reference(args, rank, world):
                  "config": {"workload": "two-surface operator application solve_IE_1step, h=1/64, KITC P=6 N0=2000 theta=0.6",
                             "pairs_per_step": n_pairs},
                  "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
-                                  "kind": "reference",
+                                  "kind": "reference", "cpu_model": cpu_model(),
                                   "sample": "%d reference matvecs (solve_IE_1step) at h=1/64" % args.steps},
                  "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
     print(json.dumps(line))
@@ -469,10 +489,15 @@ def run_ours(args, rank, world, local_rank):
         if world == 1 and not args.no_cpu_baseline:
             try:
                 os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-                _, dt = cpu_reference_matvec(None)
+                _, dt, dt_sums = cpu_reference_matvec(None)
                 cpu = {"value": pairs_of(w_mv) / dt, "unit": "pairs/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
-                       "kind": "reference",
-                       "sample": "one reference operator application (solve_IE_1step, h=1/%d, P=%d, N0=%d), %.1f s" % (H_INV, P, N0, dt)}
+                       "kind": "reference", "cpu_model": cpu_model(),
+                       "sample": "one reference operator application (solve_IE_1step, h=1/%d, P=%d, N0=%d), %.1f s" % (H_INV, P, N0, dt),
+                       # kernel for kernel: the same pairs through the reference's four stresslet
+                       # treecode sums alone (its operator also runs a serial nearest-point
+                       # interpolation search each call, which the plan here does once)
+                       "sums_only": {"value": pairs_of(w_mv) / dt_sums, "unit": "pairs/s", "seconds": dt_sums,
+                                     "gpu_batch_pairs_per_s": pairs_of(w_mv) / (ms_dl * 1e-3)}}
             except Exception as e:  # reference build absent
                 cpu = {"value": None, "unit": "pairs/s", "cores": 0, "kind": "reference",
                        "sample": "unavailable: %s" % e}
