@@ -37,6 +37,7 @@ namespace {
 
 constexpr int kDstLines = 8;      // lines per CTA (consecutive doubles per rotated store)
 constexpr int kDstThreads = 256;  // eight warps: one line per warp in the split step
+constexpr int kDstRegLines = 16;  // lines per CTA of the register pass (two per warp)
 constexpr int kDstMaxStages = 24;
 
 // Radices of the length-P complex FFT, in stage order.
@@ -329,23 +330,33 @@ __global__ void __launch_bounds__(kDstThreads, 4)
 
 // ------------------------------------------------------------------------
 // Register DST-I pass for lines of n = 64 R - 1 points (N = 64 R, complex
-// length P = 32 R; R = 2, 3, 4, 6, 8: the N = 384 grid is R = 6): one warp
-// per line, the complex sequence held as R values per lane (element
-// m = 32 a + bitrev5(b) in register a of lane b), so the FFT runs in
-// registers and warp shuffles and shared memory only stages the rotated store.
+// length P = 32 R; R = 2, 3, 4, 6, 8: the N = 384 grid is R = 6): a CTA of
+// eight warps takes kDstRegLines = 16 consecutive lines, two per warp in
+// turn; a warp holds one line's complex sequence as R values per lane (element
+// m = 32 a + b in register a of lane b), so the FFT runs in registers and
+// warp shuffles and shared memory only stages the rotated store.
 //   1. y_j of the auxiliary-array method, read straight from global memory
-//      (lane b needs x_j, x_{j+1} and their mirrors for j = 64 a + 2 m_b; a
-//      warp's reads cover 64 consecutive points per a, in a permuted order);
+//      (lane b needs x_j, x_{j+1} and their mirrors for j = 64 a + 2 b: a
+//      warp's reads cover 64 consecutive points per a in lane order, which
+//      takes fewer L1 wavefronts than the same addresses in a permuted lane
+//      order);
 //   2. P = R x 32: an R-point DFT over each lane's registers, the twiddles
-//      W_P^{m_b k1}, then a 32-point decimation-in-time DFT across the lanes
-//      (five butterfly stages with shuffles; bit-reversed input, natural
-//      output), leaving Z_{k1 + R b} in register k1 of lane b;
+//      W_P^{b k1}, then a 32-point decimation-in-frequency DFT across the
+//      lanes (five butterfly stages with shuffles; natural input,
+//      bit-reversed output), leaving Z_{k1 + R m_b} in register k1 of lane b
+//      (m_b = bitrev5(b));
 //   3. the real split with the partner Z_{P-k} fetched by one shuffle per
 //      register (lane b ^ 31 for k1 > 0), and the odd-output recurrence as an
-//      in-lane prefix over k1 plus a warp scan over the lanes;
-//   4. the CTA's kDstLines lines written rotated through shared memory (even
-//      and odd outputs in separate regions: lanes' stores two-way at most)
-//      with the pass's epilogue, as in dst_pass_kernel.
+//      in-lane prefix over k1 plus a warp scan over the lanes' totals put in
+//      k order;
+//   4. the CTA's 16 lines written rotated through shared memory (even and
+//      odd outputs in separate regions: lanes' stores two-way at most) with
+//      the pass's epilogue, as in dst_pass_kernel: 16 consecutive doubles,
+//      one 128-byte segment, per output index.
+// Every sine and twiddle factor a lane uses depends only on its lane index,
+// so the pass reads them from a lane-major table (item i of lane b at
+// 32 i + b, one coalesced 512-byte row per item) rather than gathering them
+// from the length-N tables: dst_reg_items(R) rows, laid out by dst_reg_table.
 
 __device__ __forceinline__ void dft6(double2* v) {
   // 6 = 2 x 3: DFTs of the even and the odd elements, then W6^k
@@ -375,6 +386,32 @@ __device__ __forceinline__ void dft_regs(double2* v) {
 
 __device__ __forceinline__ int brev5(int x) { return (int)(__brev((unsigned)x) >> 27); }
 
+// Rows of the register pass's lane-major table, for lane b (m_b = bitrev5(b)):
+//   a = 0..R-1          (sin(j pi/N), sin((j+1) pi/N)), j = 64 a + 2 b
+//   R - 1 + k1, k1 > 0  W_P^{b k1}
+//   2R - 2 + log2 s     W_{2s}^{b mod s}, s = 2, 4, 8, 16 (the lane-DFT stages)
+//   2R + 3 + k1         e^{-2 pi i k/N}, k = k1 + R m_b (the real split)
+constexpr int dst_reg_items(int R) { return 3 * R + 3; }
+
+// Fills the lane-major table of the register pass from the length-N tables
+// tw[k] = e^{-2 pi i k/N} and st[k] = sin(k pi/N) (N = 64 R).
+std::vector<double2> dst_reg_table(int R, const std::vector<double2>& tw, const std::vector<double>& st) {
+  const int N = 64 * R;
+  std::vector<double2> t((size_t)dst_reg_items(R) * 32);
+  for (int b = 0; b < 32; b++) {
+    int mb = 0;
+    for (int i = 0; i < 5; i++) mb |= ((b >> i) & 1) << (4 - i);
+    for (int a = 0; a < R; a++) {
+      const int j = 64 * a + 2 * b;
+      t[(size_t)a * 32 + b] = make_double2(st[j], st[j + 1]);
+    }
+    for (int k1 = 1; k1 < R; k1++) t[(size_t)(R - 1 + k1) * 32 + b] = tw[2 * b * k1];
+    for (int l = 1, s = 2; s <= 16; l++, s <<= 1) t[(size_t)(2 * R - 2 + l) * 32 + b] = tw[(b & (s - 1)) * (N / (2 * s))];
+    for (int k1 = 0; k1 < R; k1++) t[(size_t)(2 * R + 3 + k1) * 32 + b] = tw[k1 + R * mb];
+  }
+  return t;
+}
+
 __device__ __forceinline__ double2 shfl2(double2 v, int src) {
   return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
@@ -386,32 +423,41 @@ __global__ void __launch_bounds__(kDstThreads, 3)
                         const double* __restrict__ evc, const double* __restrict__ evs, double scale,
                         const double* __restrict__ w, double* __restrict__ u) {
   extern __shared__ __align__(16) double dsm[];
-  constexpr int T = kDstLines;
+  constexpr int T = kDstRegLines;
   constexpr int RS = T + 1;
   constexpr int P = 32 * R, N = 2 * P, n = N - 1;
-  static_assert(kDstThreads == 32 * T, "one warp per line");
+  constexpr int W = kDstThreads / 32;  // warps; warp wp takes lines wp, wp + W, ...
+  static_assert(T % W == 0 && kDstThreads % T == 0, "whole lines per warp, a fixed line per storing thread");
   const long lines = (long)n * n;
   const long l0 = (long)blockIdx.x * T;
   const int nt = (int)min((long)T, lines - l0);
-  const int t = threadIdx.x >> 5, b = threadIdx.x & 31;
-  const bool live = t < nt;
+  const int wp = threadIdx.x >> 5, b = threadIdx.x & 31;
   const int mb = brev5(b);
 
-  // 1. z_m = y_{2m} + i y_{2m+1}, m = 32 a + bitrev5(b)
+  // the lane-major table (tw points at it for this pass): row i at lt[32 i]
+  const double2* lt = tw + b;
+
+  double* E = dsm;
+  double* O = dsm + P * RS;
+#pragma unroll 1
+  for (int t = wp; t < T; t += W) {
+  const bool live = t < nt;
+  // 1. z_m = y_{2m} + i y_{2m+1}, m = 32 a + b
   double2 z[R];
   {
     const double* row = in + (l0 + (live ? t : 0)) * n;
 #pragma unroll
     for (int a = 0; a < R; a++) {
-      const int j = 64 * a + 2 * mb;
+      const int j = 64 * a + 2 * b;
+      const double2 sn = __ldg(&lt[32 * a]);  // sin(j pi/N), sin((j+1) pi/N)
       double yr = 0.0, yi = 0.0;
       if (live) {
         if (j > 0) {
           const double xj = row[j - 1], xm = row[N - j - 1];
-          yr = __ldg(&sintab[j]) * (xj + xm) + 0.5 * (xj - xm);
+          yr = sn.x * (xj + xm) + 0.5 * (xj - xm);
         }
         const double xj1 = row[j], xm1 = row[N - j - 2];
-        yi = __ldg(&sintab[j + 1]) * (xj1 + xm1) + 0.5 * (xj1 - xm1);
+        yi = sn.y * (xj1 + xm1) + 0.5 * (xj1 - xm1);
       }
       z[a] = make_double2(yr, yi);
     }
@@ -420,43 +466,44 @@ __global__ void __launch_bounds__(kDstThreads, 3)
   // 2. Z_{k1 + R k2} = sum_m2 W32^{m2 k2} W_P^{m2 k1} sum_a z_{32 a + m2} W_R^{a k1}
   dft_regs<R>(z);
 #pragma unroll
-  for (int k1 = 1; k1 < R; k1++) z[k1] = cmul(z[k1], __ldg(&tw[2 * mb * k1]));  // W_P^x = tw[2x]
+  for (int k1 = 1; k1 < R; k1++) z[k1] = cmul(z[k1], __ldg(&lt[32 * (R - 1 + k1)]));  // W_P^{b k1}
 #pragma unroll
-  for (int s = 1; s <= 16; s <<= 1) {
-    // radix-2 DIT across lanes: pair (L, L + s) with a = x_L, c = x_{L+s},
-    // omega = W_{2s}^{L mod s}: x_L = a + omega c, x_{L+s} = a - omega c
+  for (int s = 16, l = 4; s >= 1; s >>= 1, l--) {
+    // radix-2 DIF across lanes: pair (L, L + s) with u = x_L, v = x_{L+s}:
+    // x_L = u + v, x_{L+s} = (u - v) W_{2s}^{L mod s}
     const bool upper = (b & s) != 0;
-    const double sg = upper ? -1.0 : 1.0;
-    const double2 om = s > 1 ? __ldg(&tw[(b & (s - 1)) * (N / (2 * s))]) : make_double2(1.0, 0.0);
+    const double2 om = s > 1 ? __ldg(&lt[32 * (2 * R - 2 + l)]) : make_double2(1.0, 0.0);
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++) {
       const double2 p = make_double2(__shfl_xor_sync(0xffffffffu, z[k1].x, s),
                                      __shfl_xor_sync(0xffffffffu, z[k1].y, s));
-      const double2 c = upper ? z[k1] : p;   // the upper element
-      const double2 a0 = upper ? p : z[k1];  // the lower element
-      const double2 oc = s > 1 ? cmul(c, om) : c;
-      z[k1] = make_double2(fma(sg, oc.x, a0.x), fma(sg, oc.y, a0.y));
+      if (!upper) {
+        z[k1] = cadd(z[k1], p);
+      } else {
+        const double2 d = csub(p, z[k1]);
+        z[k1] = s > 1 ? cmul(d, om) : d;
+      }
     }
   }
-  // lane b now holds Z_k, k = k1 + R b
+  // lane b now holds Z_k, k = k1 + R bitrev5(b)
 
   // 3. real split: partner Z_{P - k}: k1 > 0 -> register R - k1 of lane b ^ 31;
-  //    k1 = 0 -> register 0 of lane (32 - b) mod 32
+  //    k1 = 0 -> register 0 of the lane holding k2 = (32 - bitrev5(b)) mod 32
   double ev[R], od[R];
   {
-    const int src0 = (32 - b) & 31;
+    const int src0 = brev5((32 - mb) & 31);
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++) {
       const double2 a = z[k1];
       const double2 c = k1 == 0 ? shfl2(z[0], src0) : shfl2(z[R - k1], b ^ 31);
-      const int k = k1 + R * b;
+      const int k = k1 + R * mb;
       if (k == 0) {
         ev[k1] = a.x + a.y;  // R_0
         od[k1] = 0.0;
       } else {
         const double Ex = 0.5 * (a.x + c.x), Ey = 0.5 * (a.y - c.y);
         const double Ox = 0.5 * (a.y + c.y), Oy = -0.5 * (a.x - c.x);
-        const double2 wk = __ldg(&tw[k]);
+        const double2 wk = __ldg(&lt[32 * (2 * R + 3 + k1)]);  // e^{-2 pi i k/N}
         const double Yx = Ex + (wk.x * Ox - wk.y * Oy);
         const double Yy = Ey + (wk.x * Oy + wk.y * Ox);
         ev[k1] = 2.0 * Yx;   // summed into the even outputs below
@@ -464,59 +511,68 @@ __global__ void __launch_bounds__(kDstThreads, 3)
       }
     }
   }
-  // even outputs: 2F at 2k = R_0 + sum_{k' = 1..k} 2 Yx_{k'} (natural order k = k1 + R b)
+  // even outputs: 2F at 2k = R_0 + sum_{k' = 1..k} 2 Yx_{k'} in natural order of
+  // k = k1 + R k2: a prefix over k1 in each lane, then over the lanes' totals
+  // in k2 order (gathered to lane k2, scanned, returned to lane bitrev5(k2))
   {
 #pragma unroll
     for (int k1 = 1; k1 < R; k1++) ev[k1] += ev[k1 - 1];
-    double incl = ev[R - 1];
+    const double tn = __shfl_sync(0xffffffffu, ev[R - 1], mb);  // total of k2 = b
+    double incl = tn;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
       const double x = __shfl_up_sync(0xffffffffu, incl, d);
       if (b >= d) incl += x;
     }
-    const double excl = incl - ev[R - 1];
+    const double excl = __shfl_sync(0xffffffffu, incl - tn, mb);  // for k2 = bitrev5(b)
 #pragma unroll
     for (int k1 = 0; k1 < R; k1++) ev[k1] += excl;
   }
   // stage the outputs: even 2k at E[k], odd 2k - 1 at O[k - 1] (columns: lines)
-  double* E = dsm;
-  double* O = dsm + P * RS;
 #pragma unroll
   for (int k1 = 0; k1 < R; k1++) {
-    const int k = k1 + R * b;
+    const int k = k1 + R * mb;
     E[k * RS + t] = ev[k1];
     if (k > 0) O[(k - 1) * RS + t] = od[k1];
   }
+  }  // lines of this warp
   __syncthreads();
 
-  // 4. rotated stores with the pass's epilogue (as dst_pass_kernel)
-  for (int idx = threadIdx.x; idx < n * T; idx += kDstThreads) {
-    const int kk = idx / T, tt = idx - kk * T;
-    if (tt >= nt) continue;
-    const long l = l0 + tt;
+  // 4. rotated stores with the pass's epilogue (as dst_pass_kernel). A thread
+  //    always stores line tt (kDstThreads is a multiple of T), so the line's
+  //    grid position and eigenvalue factors are formed once, outside the loop.
+  const int tt = threadIdx.x % T;
+  if (tt >= nt) return;
+  const long l = l0 + tt;
+  const int ja = (int)(l / n), jb = (int)(l - (long)ja * n);
+  double ca = 0.0, sa = 0.0, cb = 0.0, sb = 0.0;
+  if (mode == 1) {
+    ca = __ldg(&evc[ja]);
+    sa = __ldg(&evs[ja]);
+    cb = __ldg(&evc[jb]);
+    sb = __ldg(&evs[jb]);
+  }
+  constexpr long M = n + 2;  // grid size N_grid + 1
+  const long g0 = ((long)M + (ja + 1)) * M + (jb + 1);  // u, w at output 0 of this line
+  for (int kk = threadIdx.x / T; kk < n; kk += kDstThreads / T) {
     const double F2 = (kk & 1) ? O[(kk >> 1) * RS + tt] : E[(kk >> 1) * RS + tt];
     if (mode == 0) {
       out[kk * lines + l] = F2;
     } else if (mode == 3) {
       out[kk * lines + l] = F2 * scale;
+    } else if (mode == 1) {
+      // eigenvalue factors in the order E2G/main.cpp:1445-1460 forms them
+      const double c1 = __ldg(&evc[kk]), s1 = __ldg(&evs[kk]);
+      const double lap7 = s1 + sa + sb;
+      const double sum8 = c1 * ca * cb;
+      const double factor = 2.0 / 3.0 * (2.0 * lap7 + sum8 - 1.0);
+      double v = F2;
+      if (fabs(factor) > 1.e-14) v /= factor;
+      else v = 0.0;
+      out[kk * lines + l] = v;
     } else {
-      const int ja = (int)(l / n), jb = (int)(l - (long)ja * n);
-      if (mode == 1) {
-        const double c1 = __ldg(&evc[kk]), s1 = __ldg(&evs[kk]);
-        const double ca = __ldg(&evc[ja]), sa = __ldg(&evs[ja]);
-        const double cb = __ldg(&evc[jb]), sb = __ldg(&evs[jb]);
-        const double lap7 = s1 + sa + sb;
-        const double sum8 = c1 * ca * cb;
-        const double factor = 2.0 / 3.0 * (2.0 * lap7 + sum8 - 1.0);
-        double v = F2;
-        if (fabs(factor) > 1.e-14) v /= factor;
-        else v = 0.0;
-        out[kk * lines + l] = v;
-      } else {
-        const long M = n + 2;  // grid size N_grid + 1
-        const long gi = ((long)(kk + 1) * M + (ja + 1)) * M + (jb + 1);
-        u[gi] = w[gi] + F2 * scale;
-      }
+      const long gi = g0 + (long)kk * M * M;
+      u[gi] = w[gi] + F2 * scale;
     }
   }
 }
@@ -653,8 +709,9 @@ struct DstPlan {
   size_t smem = 0;
   DstRadix rad{};
   PassFn fn = nullptr;
+  int reg_R = 0;  // lines of 64 R - 1 points run the register pass
   DBuf<double> sintab, evc, evs, tmp;
-  DBuf<double2> tw;
+  DBuf<double2> tw, lanetab;
   void make(Ctx& C, int n_) {
     n = n_;
     const int N = n + 1;
@@ -673,10 +730,12 @@ struct DstPlan {
     // register pass; the other benchmark sizes (N = 48, 96) passes compiled
     // for their line length; any other the general shared-memory pass
     const int R = P % 32 == 0 ? P / 32 : 0;
+    reg_R = 0;
     if (R == 2 || R == 3 || R == 4 || R == 6 || R == 8) {
+      reg_R = R;
       fn = R == 2 ? dst_pass_reg_kernel<2> : R == 3 ? dst_pass_reg_kernel<3> : R == 4 ? dst_pass_reg_kernel<4>
          : R == 6 ? dst_pass_reg_kernel<6> : dst_pass_reg_kernel<8>;
-      smem = (size_t)(n + 1) * (kDstLines + 1) * sizeof(double);  // P rows of even, P of odd outputs
+      smem = (size_t)(n + 1) * (kDstRegLines + 1) * sizeof(double);  // P rows of even, P of odd outputs
     } else {
       fn = P == 48 ? dst_pass_kernel<48> : P == 24 ? dst_pass_kernel<24> : dst_pass_kernel<0>;
       smem = 2 * (size_t)dst_bufd(P) * sizeof(double);
@@ -704,15 +763,18 @@ struct DstPlan {
     }
     tw.upload(t, C.stream);
     sintab.upload(st, C.stream);
+    if (reg_R) lanetab.upload(dst_reg_table(reg_R, t, st), C.stream);
     evc.upload(c, C.stream);
     evs.upload(s, C.stream);
   }
   // one pass: in [n][n][n] -> out rotated (or into u for mode 2)
   void pass(Ctx& C, const double* in, double* out, int mode, double scale, const double* w, double* u) {
     const long lines = (long)n * n;
-    const long blocks = (lines + kDstLines - 1) / kDstLines;
-    fn<<<(unsigned)blocks, kDstThreads, smem, C.stream>>>(n, rad, in, out, mode, tw.p, sintab.p, evc.p, evs.p,
-                                                          scale, w, u);
+    const int per_cta = reg_R ? kDstRegLines : kDstLines;
+    const long blocks = (lines + per_cta - 1) / per_cta;
+    // the register pass takes its lane-major table in place of the twiddles
+    fn<<<(unsigned)blocks, kDstThreads, smem, C.stream>>>(n, rad, in, out, mode, reg_R ? lanetab.p : tw.p,
+                                                          sintab.p, evc.p, evs.p, scale, w, u);
     C.launches++;
     HR_CHECK_CUDA(cudaGetLastError());
   }
