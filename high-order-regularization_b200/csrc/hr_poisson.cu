@@ -350,9 +350,10 @@ __global__ void __launch_bounds__(kDstThreads, 4)
 //      in-lane prefix over k1 plus a warp scan over the lanes' totals put in
 //      k order;
 //   4. the CTA's 16 lines written rotated through shared memory (even and
-//      odd outputs in separate regions: lanes' stores two-way at most) with
-//      the pass's epilogue, as in dst_pass_kernel: 16 consecutive doubles,
-//      one 128-byte segment, per output index.
+//      odd outputs in separate regions, columns rotated per row group so that
+//      the stores of a half-warp meet 16 distinct banks) with the pass's
+//      epilogue, as in dst_pass_kernel: 16 consecutive doubles, one 128-byte
+//      segment, per output index.
 // Every sine and twiddle factor a lane uses depends only on its lane index,
 // so the pass reads them from a lane-major table (item i of lane b at
 // 32 i + b, one coalesced 512-byte row per item) rather than gathering them
@@ -385,6 +386,12 @@ __device__ __forceinline__ void dft_regs(double2* v) {
 }
 
 __device__ __forceinline__ int brev5(int x) { return (int)(__brev((unsigned)x) >> 27); }
+
+// Column rotation of staging row group x (rows x R .. x R + R - 1): the 16
+// lanes of a half-warp, whose groups are the even or the odd x, then store to
+// 16 distinct banks.
+template <int R, int RS>
+__device__ __forceinline__ int dst_swz(int x) { return ((x >> 1) - ((R * RS) & 15) * x) & 15; }
 
 // Rows of the register pass's lane-major table, for lane b (m_b = bitrev5(b)):
 //   a = 0..R-1          (sin(j pi/N), sin((j+1) pi/N)), j = 64 a + 2 b
@@ -532,8 +539,8 @@ __global__ void __launch_bounds__(kDstThreads, 3)
 #pragma unroll
   for (int k1 = 0; k1 < R; k1++) {
     const int k = k1 + R * mb;
-    E[k * RS + t] = ev[k1];
-    if (k > 0) O[(k - 1) * RS + t] = od[k1];
+    E[k * RS + ((t + dst_swz<R, RS>(mb)) & (T - 1))] = ev[k1];
+    if (k > 0) O[(k - 1) * RS + ((t + dst_swz<R, RS>(k1 > 0 ? mb : mb - 1)) & (T - 1))] = od[k1];
   }
   }  // lines of this warp
   __syncthreads();
@@ -555,7 +562,8 @@ __global__ void __launch_bounds__(kDstThreads, 3)
   constexpr long M = n + 2;  // grid size N_grid + 1
   const long g0 = ((long)M + (ja + 1)) * M + (jb + 1);  // u, w at output 0 of this line
   for (int kk = threadIdx.x / T; kk < n; kk += kDstThreads / T) {
-    const double F2 = (kk & 1) ? O[(kk >> 1) * RS + tt] : E[(kk >> 1) * RS + tt];
+    const int kh = kk >> 1, col = (tt + dst_swz<R, RS>(kh / R)) & (T - 1);
+    const double F2 = (kk & 1) ? O[kh * RS + col] : E[kh * RS + col];
     if (mode == 0) {
       out[kk * lines + l] = F2;
     } else if (mode == 3) {
