@@ -239,45 +239,88 @@ Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near
   {
     std::vector<int> slot(2 * (size_t)nn, -1);
     std::vector<int> touched;
-    std::vector<int> stack;
     std::vector<std::vector<int>> keys(kTB);  // each target's entries, in traversal order
     std::vector<int> order(kTB), tsave(kTB);
+    std::vector<double> tx(kTB), ty(kTB), tz(kTB);
+    std::vector<uint8_t> treg(kTB);
+    std::vector<std::vector<int>> sub(2, std::vector<int>(kTB));  // targets reaching a node, per depth
 #pragma omp for schedule(dynamic, 4)
     for (int b = 0; b < nb; b++) {
       std::vector<Entry>& E = per[b];
       touched.clear();
       const int cnt_t = std::min(kTB, nt - b * kTB);
+      // One depth-first traversal per block carries the block's targets that
+      // reach each node. A node whose centre is farther from the block's
+      // bounding box than its MAC radius is far for all of them, and one that
+      // holds the whole box within it is far for none: rounding is monotone, so
+      // every target's R_sq lies between the box's rounded extremes (a 1e-13
+      // margin on top). Only the other nodes test targets one by one, with the
+      // per-target expression. A target's keys come out in the per-target
+      // traversal's order (children in order), so the lists are unchanged.
+      double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
       for (int tt = 0; tt < cnt_t; tt++) {
         keys[tt].clear();
-        int k = b * kTB + tt;
-        int t = L.tord[k];
-        const double px = txyz[3 * t], py = txyz[3 * t + 1], pz = txyz[3 * t + 2];
-        bool regt = near ? near[t] != 0 : true;
-        stack.clear();
-        stack.push_back(0);
-        while (!stack.empty()) {
-          int c = stack.back();
-          stack.pop_back();
-          double tpx = px - T.xc[c], tpy = py - T.yc[c], tpz = pz - T.zc[c];
-          double R_sq = tpx * tpx + tpy * tpy + tpz * tpz;
-          int type;
-          if (T.mac[c] < R_sq) {
-            type = 0;
-            prox[b] += Pf;
-          } else if ((T.m1[c] - T.m0[c]) < T.N0 || T.child_count[c] == 0) {
-            type = 1;
-            long long cnt = T.m1[c] - T.m0[c] + 1;
-            if (regt) reg[b] += cnt;
-            else plain[b] += cnt;
-          } else {
-            // children in reverse so that they pop in the reference's order
-            for (int q = T.child_count[c] - 1; q >= 0; q--)
-              stack.push_back(T.children[T.child_start[c] + q]);
-            continue;
-          }
-          keys[tt].push_back(2 * c + type);
+        const int t = L.tord[b * kTB + tt];
+        tx[tt] = txyz[3 * t];
+        ty[tt] = txyz[3 * t + 1];
+        tz[tt] = txyz[3 * t + 2];
+        treg[tt] = near ? near[t] != 0 : true;
+        const double v[3] = {tx[tt], ty[tt], tz[tt]};
+        for (int d = 0; d < 3; d++) {
+          bmin[d] = tt == 0 ? v[d] : std::min(bmin[d], v[d]);
+          bmax[d] = tt == 0 ? v[d] : std::max(bmax[d], v[d]);
         }
       }
+      for (int tt = 0; tt < cnt_t; tt++) sub[0][tt] = tt;
+      auto visit = [&](auto&& self, int c, int depth, int ns) -> void {
+        const int* S = sub[depth].data();
+        const double ctr[3] = {T.xc[c], T.yc[c], T.zc[c]};
+        double lo[3], hi[3];
+        for (int d = 0; d < 3; d++) {
+          lo[d] = ctr[d] < bmin[d] ? bmin[d] - ctr[d] : (ctr[d] > bmax[d] ? ctr[d] - bmax[d] : 0.0);
+          hi[d] = std::max(std::fabs(bmin[d] - ctr[d]), std::fabs(bmax[d] - ctr[d]));
+        }
+        const double dmin2 = lo[0] * lo[0] + lo[1] * lo[1] + lo[2] * lo[2];
+        const double dmax2 = hi[0] * hi[0] + hi[1] * hi[1] + hi[2] * hi[2];
+        const bool leaf = (T.m1[c] - T.m0[c]) < T.N0 || T.child_count[c] == 0;
+        const long long cnt = T.m1[c] - T.m0[c] + 1;
+        if (T.mac[c] < dmin2 * (1.0 - 1e-13)) {  // far for every target
+          for (int e = 0; e < ns; e++) keys[S[e]].push_back(2 * c);
+          prox[b] += Pf * ns;
+          return;
+        }
+        int nr = ns;
+        const int* Rr = S;
+        if (!(T.mac[c] >= dmax2 * (1.0 + 1e-13))) {  // mixed: the per-target test
+          if ((int)sub.size() <= depth + 1) sub.emplace_back(kTB);
+          int* W = sub[depth + 1].data();
+          nr = 0;
+          for (int e = 0; e < ns; e++) {
+            const int tt = S[e];
+            double tpx = tx[tt] - T.xc[c], tpy = ty[tt] - T.yc[c], tpz = tz[tt] - T.zc[c];
+            double R_sq = tpx * tpx + tpy * tpy + tpz * tpz;
+            if (T.mac[c] < R_sq) {
+              keys[tt].push_back(2 * c);
+              prox[b] += Pf;
+            } else {
+              W[nr++] = tt;
+            }
+          }
+          Rr = W;
+          if (nr == 0) return;
+        }
+        if (leaf) {
+          for (int e = 0; e < nr; e++) {
+            keys[Rr[e]].push_back(2 * c + 1);
+            if (treg[Rr[e]]) reg[b] += cnt;
+            else plain[b] += cnt;
+          }
+          return;
+        }
+        const int nd = Rr == S ? depth : depth + 1;
+        for (int q = 0; q < T.child_count[c]; q++) self(self, T.children[T.child_start[c] + q], nd, nr);
+      };
+      visit(visit, 0, 0, cnt_t);
       // Targets with the same (or a similar) interaction list take neighbouring
       // positions, so that a warp's 32 targets tend to share their entries and
       // warps skip more entries whole. A target's sums do not depend on its
