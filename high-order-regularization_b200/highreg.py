@@ -106,6 +106,8 @@ def lib():
         L.hr_plan2s_destroy.restype = None
         L.hr_ctx_destroy.restype = None
         L.hr_dst1_plan_destroy.restype = None
+        L.hr_host_free.restype = None
+        L.hr_host_free.argtypes = [ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -120,6 +122,22 @@ def _i32(a):
 
 def _dp(a):
     return None if a is None else a.ctypes.data_as(_D)
+
+
+def pinned_empty(n, dtype=np.float64):
+    """An uninitialised 1-D numpy array of n elements in page-locked host memory
+    (hr_host_alloc), freed with the array. Copies between it and the device run
+    at DMA speed, without the staging that pageable memory needs."""
+    dtype = np.dtype(dtype)
+    nbytes = max(1, int(n) * dtype.itemsize)
+    ptr = ctypes.c_void_p()
+    rc = lib().hr_host_alloc(ctypes.c_size_t(nbytes), ctypes.byref(ptr))
+    if rc != HR_OK:
+        raise HrError(rc, "hr_host_alloc of %d bytes failed" % nbytes)
+    buf = (ctypes.c_char * nbytes).from_address(ptr.value)
+    arr = np.frombuffer(buf, dtype=dtype, count=int(n))
+    weakref.finalize(buf, lib().hr_host_free, ptr.value)
+    return arr
 
 
 def _ip(a):
@@ -576,9 +594,15 @@ class E2G:
         self.ctx._check(lib().hr_e2g_run(self.p, precision, ctypes.byref(rep)))
         return {k: getattr(rep, k) for k, _ in E2GReport._fields_}
 
-    def get(self, which):
+    def get(self, which, out=None):
+        """Grid `which` of the last run (hr_e2g_get) as float64. `out`, if
+        given (e.g. from pinned_empty), is filled in place and returned."""
         m = (self.N + 1) ** 3
-        out = np.zeros(3 * m if which in (1, 3) else m)
+        n = 3 * m if which in (1, 3) else m
+        if out is None:
+            out = np.empty(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise HrError(HR_ERR_ARG, "E2G.get: out must be a contiguous float64 array of %d elements" % n)
         self.ctx._check(lib().hr_e2g_get(self.p, which, _dp(out)))
         return out
 

@@ -46,6 +46,19 @@ def test_pipeline_matches_reference(e48, ge2g):
     assert e32 < 1e-3
 
 
+def test_read_back_into_page_locked_buffer(e48):
+    # the same grids through a caller's page-locked buffer, filled in place
+    e48.run()
+    ref = e48.get(3)
+    buf = highreg.pinned_empty(ref.size)
+    buf[:] = np.nan
+    got = e48.get(3, out=buf)
+    assert got is buf and np.array_equal(got, ref)
+    assert np.array_equal(e48.get(2, out=highreg.pinned_empty(ref.size // 3)), e48.get(2))
+    with pytest.raises(highreg.HrError):
+        e48.get(3, out=highreg.pinned_empty(ref.size - 1))
+
+
 def _exact_grids(N, h):
     M = N + 1
     p = np.zeros(M ** 3)
