@@ -37,6 +37,31 @@ __global__ void scatter_kernel(int n, int comps, const long* __restrict__ gi,
   }
 }
 
+// The Poisson masks (E2G/main.cpp:1611-1614, 1654-1672): band2 is set
+// beforehand at the BAND2 points (scattered from the tagged targets); a point
+// is exterior when phi(x) > 0 and it is not in BAND2. The level set is formed
+// with unfused operations in the order the host's expression
+// u0 u0 / 1 + u1 u1 / 0.25 + u2 u2 / 0.25 - 1 evaluates (dividing by 0.25 is
+// multiplying by 4 exactly), so the sign test is the host's.
+__global__ void exterior_mask_kernel(int M, double h, const uint8_t* __restrict__ band2, uint8_t* __restrict__ om) {
+  const long m3 = (long)M * M * M;
+  for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < m3; g += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(g / ((long)M * M)), j = (int)((g / M) % M), k = (int)(g % M);
+    const double u0 = __dsub_rn(__dmul_rn((double)i, h), 1.5);
+    const double u1 = __dsub_rn(__dmul_rn((double)j, h), 1.5);
+    const double u2 = __dsub_rn(__dmul_rn((double)k, h), 1.5);
+    const double levl = __dsub_rn(__dadd_rn(__dadd_rn(__dmul_rn(u0, u0), __dmul_rn(__dmul_rn(u1, u1), 4.0)),
+                                            __dmul_rn(__dmul_rn(u2, u2), 4.0)),
+                                  1.0);
+    om[g] = (levl > 0.0 && !band2[g]) ? 1 : 0;
+  }
+}
+
+__global__ void set_points_kernel(int n, const long* __restrict__ gi, uint8_t* __restrict__ mask) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) mask[gi[t]] = 1;
+}
+
 constexpr double kPI = 3.14159265358979323846;
 
 // ---------------------------------------------------------------- error norms
@@ -367,23 +392,22 @@ extern "C" int hr_e2g_create(hr_ctx* ctx, int N, hr_e2g** out) {
     E->ub.alloc(3 * (size_t)std::max(1, E->nband));
     e2g_batch(*E, HR_FP64, C);  // the reduced-precision batches are built on first use
     E->pairs = 2LL * (E->nface + E->nband) * (long long)surf.n;
-    // masks: BAND2 points, and exterior points outside BAND2 (E2G/main.cpp:1611-1614, 1654-1672)
-    std::vector<uint8_t, e2g_setup::NoInitAlloc<uint8_t>> b2((size_t)M * M * M), om((size_t)M * M * M);
-#pragma omp parallel for schedule(static)
-    for (int i = 0; i < M; i++)
-      for (int j = 0; j < M; j++)
-        for (int k = 0; k < M; k++) {
-          long g = ((long)i * M + j) * M + k;
-          int ind = S.nrst[g];
-          const bool in2 = ind != -1 && S.band2[ind];
-          b2[g] = in2 ? 1 : 0;
-          double x[3] = {i * h, j * h, k * h};
-          double u0 = x[0] - 1.5, u1 = x[1] - 1.5, u2 = x[2] - 1.5;
-          double levl = u0 * u0 / 1.0 + u1 * u1 / 0.25 + u2 * u2 / 0.25 - 1.0;
-          om[g] = (levl > 0 && !in2) ? 1 : 0;
-        }
-    E->mband2.upload(b2.data(), b2.size(), st);
-    E->mout.upload(om.data(), om.size(), st);
+    // masks: BAND2 points, and exterior points outside BAND2, built on the
+    // device from the BAND2 targets' grid indices
+    const size_t mm = (size_t)M * M * M;
+    std::vector<long> g2;
+    for (size_t t = 0; t < S.band2.size(); t++)
+      if (S.band2[t]) g2.push_back(S.g[t]);
+    DBuf<long> dg2;
+    dg2.upload(g2, st);
+    E->mband2.alloc(mm);
+    E->mband2.zero(st);
+    E->mout.alloc(mm);
+    if (!g2.empty())
+      set_points_kernel<<<(unsigned)((g2.size() + 255) / 256), 256, 0, st>>>((int)g2.size(), dg2.p, E->mband2.p);
+    exterior_mask_kernel<<<4 * C.num_sms, 256, 0, st>>>(M, h, E->mband2.p, E->mout.p);
+    C.launches += 2;
+    HR_CHECK_CUDA(cudaGetLastError());
     size_t m3 = (size_t)M * M * M;
     E->p_bi.alloc(m3);
     E->u_bi.alloc(3 * m3);

@@ -468,10 +468,12 @@ void build(Scene& S, int N, double band1, double band2) {
   S.x0.resize(3 * nkept);
   S.n0.resize(3 * nkept);
   S.band2.resize(nkept);
+  S.g.resize(nkept);
 #pragma omp parallel for schedule(static)
   for (long t = 0; t < nkept; t++) {
     const Tag& T = kept[t];
     S.nrst[T.g] = (int)t;
+    S.g[t] = T.g;
     S.b[t] = T.b;
     for (int d = 0; d < 3; d++) {
       S.x0[3 * t + d] = T.x0[d];

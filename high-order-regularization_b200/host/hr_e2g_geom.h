@@ -35,6 +35,7 @@ struct Scene {
   std::vector<double> xq, nrm, area, f;  // quadrature points, normals, areas, exact density
   std::vector<int, NoInitAlloc<int>> nrst;  // (N+1)^3: tagged target index or -1
   std::vector<double> b, x0, n0;         // per tagged target
+  std::vector<long> g;                   // grid index of each tagged target
   std::vector<uint8_t> band2;
 };
 
