@@ -162,6 +162,55 @@ def cpu_reference_matvec(geo_pairs, seconds_budget=None):
     return R, dt, dt_sums
 
 
+def run_reference_solve_estimate(args, rank):
+    """The reference's CPU solve at h = 1/256 (P = 10, N0 = 8000) estimated
+    from its parts, for the GPU solve times the default run reports: the
+    reference's right-hand side eval_SL once and its operator application
+    solve_IE_1step once (with, alone, its serial interpolate_DL_density and
+    its four stresslet treecode sums), timed on the host cores, then
+    RHS + iterations x operator with the iteration count of the FP64 solve
+    (12 at restart 50). The scene is this library's geometry, which equals the
+    reference's own bit for bit; the reference's set-up (its O(Nt Nq)
+    nearest-point scan) is not timed. Tens of minutes of host time: not part
+    of the default run."""
+    if rank != 0:
+        return
+    import numpy as np
+
+    import highreg
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Ref2S
+
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    geo = highreg.Geometry2S(256).scene
+    R = Ref2S(10, 8000).load(geo, g=[geo["f0"], geo["f1"]])
+    t0 = time.perf_counter()
+    R.rhs()
+    t_rhs = time.perf_counter() - t0
+    u = np.random.default_rng(0).standard_normal(3 * sum(R.nq))
+    t0 = time.perf_counter()
+    R.matvec(u)
+    t_mv = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for s in (0, 1):
+        R.interpolate(s)
+    t_interp = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for s, t in ((0, 0), (0, 1), (1, 0), (1, 1)):
+        R.eval(1, True, s, t)
+    t_sums = time.perf_counter() - t0
+    iters = 12
+    est = t_rhs + iters * t_mv
+    print(json.dumps({"impl": "reference", "workload": "two-surface solve h=1/256 (n=%d), KITC P=10 N0=8000 "
+                      "theta=0.6" % (3 * sum(R.nq)), "cores": int(os.environ["OMP_NUM_THREADS"]),
+                      "cpu_model": cpu_model(), "seconds_rhs": t_rhs, "seconds_operator": t_mv,
+                      "seconds_interpolation": t_interp, "seconds_stresslet_sums": t_sums,
+                      "iterations": iters, "solve_seconds_estimated": est,
+                      "note": "RHS + 12 operator applications, each part timed once on the host cores"}))
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -646,6 +695,9 @@ def main():
     ap.add_argument("--workload", default="2s", choices=["2s", "e2g"],
                     help="2s: the two-surface solve (the benchmark); e2g: the extend-to-grid pipeline")
     ap.add_argument("--N", type=int, default=96, help="extend-to-grid grid size (96 or 384)")
+    ap.add_argument("--reference-h256-estimate", action="store_true",
+                    help="with --impl reference: time the reference's RHS and one operator application at "
+                         "h = 1/256 on the host cores and print the estimated solve time (tens of minutes)")
     ap.add_argument("--inner", default="auto",
                     help="treecode 'P,N0' of the mixed solve's inner operator; 'auto': 5,2000 when the "
                          "workload's P is above 6, 'none': no inner treecode")
@@ -668,7 +720,9 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if args.impl == "reference":
+        if args.impl == "reference" and args.reference_h256_estimate:
+            run_reference_solve_estimate(args, rank)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         elif args.workload == "e2g":
             run_e2g(args, rank, world, local_rank)
