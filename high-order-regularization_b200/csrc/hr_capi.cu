@@ -514,10 +514,15 @@ struct hr_plan2s {
   std::vector<double> hxyz[2], hnrml[2], harea[2];
   std::vector<uint8_t> near_host[2];
   hr_surface surf_host[2];
-  // The FP64 stresslet batch is segmented on a host thread of its own while
-  // the caller goes on (to the right-hand side, which needs only the Stokeslet
-  // batch), its uploads on a stream of its own; every other use of the plan
-  // first waits for it (plan_ready).
+  // the density-interpolation stencils' inputs per target set (the caller's
+  // scene need not outlive the plan's creation); built on dl_thread, then freed
+  std::vector<int> hnrst[2], hi123[2];
+  std::vector<double> hx0[2];
+  // The density-interpolation stencils are built and the FP64 stresslet batch
+  // segmented on a host thread of its own while the caller goes on (to the
+  // right-hand side, which needs only the Stokeslet batch), their uploads on a
+  // stream of its own; every other use of the plan first waits for it
+  // (plan_ready).
   std::thread dl_thread;
   std::mutex dl_mu;  // one joiner, if two host threads reach plan_ready at once
   std::exception_ptr dl_error;
@@ -612,6 +617,15 @@ void plan_batches(hr_plan2s& P) {
   P.dl_thread = std::thread([&P, dev] {
     try {
       HR_CHECK_CUDA(cudaSetDevice(dev));
+      for (int t = 0; t < 2; t++) {
+        const hr_surface& Ssrc = P.surf_host[1 - t];
+        Stencils sv = build_stencils(P.h, Ssrc.center, Ssrc.n, Ssrc.xyz, P.nq[t], P.hnrst[t].data(),
+                                     P.hx0[t].data(), P.hi123[t].data());
+        P.sten[t].build(sv, P.up);
+        std::vector<int>().swap(P.hnrst[t]);
+        std::vector<int>().swap(P.hi123[t]);
+        std::vector<double>().swap(P.hx0[t]);
+      }
       dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, 0, 1, true, P.up);
       HR_CHECK_CUDA(cudaEventRecord(P.up_done, P.up));
     } catch (...) {
@@ -661,6 +675,7 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
   // the reduced-precision operator runs on the inner treecode when there is one
   hr_plan2s::Inner* in = (prec != HR_FP64 && P.inner) ? P.inner.get() : nullptr;
   DevTree* trees = in ? in->tree : P.tree;
+  plan_ready(P);  // the stencils and the FP64 stresslet batch
   for (int s = 0; s < 2; s++) trees[s].set_density(C, P.xin.p + P.off[s], true, tree, prec != HR_FP64);
   for (int t = 0; t < 2; t++) {
     P.tg[t].g0.zero(st);
@@ -668,7 +683,6 @@ void plan_matvec(hr_plan2s& P, const double* x_dev, double* y_dev, int prec) {
                   P.xin.p + P.off[1 - t], P.tg[t].g0.p, st);
     C.launches++;
   }
-  plan_ready(P);
   if (!in && !P.dl[prec].ready) dl_batches(P, P.tree, P.Lon, P.Loff, P.dl, prec, prec + 1, true, st);
   (in ? in->dl[prec] : P.dl[prec]).launch(C);
   // set 0: u - on*f - comp*f ; set 1: u - comp*f - on*f   (2S/main.cpp:612-676)
@@ -965,10 +979,10 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
       std::vector<uint8_t> all(T.n, 1);
       P->Lon[t].build(P->tree[t].host, T.n, sc->surf[t].xyz, all.data(), st);
       P->Loff[t].build(P->tree[1 - t].host, T.n, sc->surf[t].xyz, near.data(), st);
-      const hr_surface& Ssrc = sc->surf[1 - t];
       check_i123(T.n, T.nrst, T.i123);
-      Stencils s = build_stencils(sc->h, Ssrc.center, Ssrc.n, Ssrc.xyz, T.n, T.nrst, T.x0, T.i123);
-      P->sten[t].build(s, st);
+      P->hnrst[t].assign(T.nrst, T.nrst + T.n);
+      P->hi123[t].assign(T.i123, T.i123 + 3 * (size_t)T.n);
+      P->hx0[t].assign(T.x0, T.x0 + 3 * (size_t)T.n);
       P->out_on[t].alloc(3 * (size_t)T.n);
       P->out_off[t].alloc(3 * (size_t)T.n);
     };
