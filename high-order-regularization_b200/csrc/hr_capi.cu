@@ -134,6 +134,7 @@ Flops flops_of(int kind) {
     case K_DL_OFF: return {129, 103, 31, 50};
     case K_E2G_SL_AWAY: return {31, 31, 31, 0};
     case K_E2G_P_AWAY: return {18, 18, 18, 0};
+    case K_E2G_UP_AWAY: return {24.5, 24.5, 24.5, 0};  // per counted pair: each fused pair counts twice
     case K_E2G_SL7: return {59, 37, 37, 0};
     default: return {64, 47, 47, 0};
   }

@@ -10,6 +10,9 @@ namespace hr {
 
 // One boundary sum: a source surface (tree order SoA) evaluated at a target
 // set (reference order). All pointers are device pointers.
+// doubles per target in a work item's partial sums (3 velocity + 1 pressure)
+constexpr int kPartComps = 4;
+
 struct EvalTask {
   int kind;       // Kind
   int jump_mode;  // DL kinds: 0 = treecode convention, 1 = direct-sum convention
@@ -37,6 +40,8 @@ struct EvalTask {
   const double *tx0, *tn0, *tg0;                      // 3nt nearest point, normal, density
   const double *tq, *tnrm;                            // 3nt own density and normal (on-surface)
   double* out;                                        // 3nt (or nt for pressure)
+  double* out2;                                       // nt pressure of K_E2G_UP_AWAY (scaled by scale2)
+  double scale2;
   const Entry* entries;                               // interaction entries
   const int* blk_start;                               // per target block, into entries
   unsigned long long* counters;  // [0] regularized pairs [1] near-target plain [2] far-target [3] proxy

@@ -265,17 +265,19 @@ static void e2g_batch(hr_e2g& E, int prec, Ctx& C) {
   const double delta = E.S.delta;
   Batch& B = E.batch[prec];
   B.family = F_E2G;
-  EvalTask a = make_task(K_E2G_P_AWAY, delta, p_scale, E.tree, E.Lf, E.tf, E.pf.p);
-  EvalTask b = make_task(K_E2G_SL_AWAY, delta, sl_scale, E.tree, E.Lf, E.tf, E.uf.p);
+  // the two box-face sums (velocity and pressure at the same targets) in one pass
+  EvalTask a = make_task(K_E2G_UP_AWAY, delta, sl_scale, E.tree, E.Lf, E.tf, E.uf.p);
+  a.out2 = E.pf.p;
+  a.scale2 = p_scale;
   EvalTask c = make_task(K_E2G_P7, delta, -p_scale, E.tree, E.Lb, E.tb, E.pb.p);
   EvalTask d = make_task(K_E2G_SL7, delta, sl_scale, E.tree, E.Lb, E.tb, E.ub.p);
-  for (EvalTask* t : {&a, &b, &c, &d}) {
+  for (EvalTask* t : {&a, &c, &d}) {
     t->mixed = prec;
     t->jump_mode = 1;
   }
-  B.tasks = {a, b, c, d};
-  B.lists = {&E.Lf.host, &E.Lf.host, &E.Lb.host, &E.Lb.host};
-  B.trees = {&E.tree.host, &E.tree.host, &E.tree.host, &E.tree.host};
+  B.tasks = {a, c, d};
+  B.lists = {&E.Lf.host, &E.Lb.host, &E.Lb.host};
+  B.trees = {&E.tree.host, &E.tree.host, &E.tree.host};
   B.finalize(C.stream, C.num_sms);
 }
 

@@ -352,6 +352,28 @@ __device__ __forceinline__ bool pair64(const double* __restrict__ sm, int j, con
   return reg;
 }
 
+// The box-face sums of one target in one pass (K_E2G_UP_AWAY):
+// stokes_SL_away and stokes_pressure_away (E2G/stokes.cpp:13-45, 102-126)
+// share the offset, the distance and f.dx, and each keeps the expression of
+// its own kind above; a3 collects the pressure.
+__device__ __forceinline__ void pair64_face(const double* __restrict__ sm, int j, const Tgt& S, double& a0,
+                                            double& a1, double& a2, double& a3) {
+  const double2* s2 = reinterpret_cast<const double2*>(sm) + 5 * j;
+  const double2 v0 = s2[0], v1 = s2[1], v3 = s2[3], v4 = s2[4];
+  const double Xj = v0.x, Yj = v0.y, Zj = v1.x, Aj = v1.y;
+  const double QXj = v3.y, QYj = v4.x, QZj = v4.y;
+  const double dx = S.px - Xj, dy = S.py - Yj, dz = S.pz - Zj;
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  const double rinv = rsqrt(r2);
+  const double fdd = QXj * dx + QYj * dy + QZj * dz;
+  const double H1 = Aj * rinv;
+  const double H2 = fdd * H1 * (rinv * rinv);
+  a0 += QXj * H1 + dx * H2;
+  a1 += QYj * H1 + dy * H2;
+  a2 += QZj * H1 + dz * H2;
+  a3 += (fdd * (rinv * rinv * rinv)) * Aj;
+}
+
 // ------------------------------------------------------- FP32 plain pairs
 // The singular kernel of each kind (the r/delta > 8 branch of the reference),
 // from FP32 centre-relative coordinates.
@@ -412,6 +434,25 @@ __device__ __forceinline__ void pair32(const float4* __restrict__ s4, int j, con
     const float tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
     p0 += (normal + tangential) * (rinv2 * rinv) * P.w;
   }
+}
+
+// The box-face sums in FP32 in one pass (as pair32 of K_E2G_SL_AWAY and of
+// K_E2G_P_AWAY, sharing the offset, the distance and f.dx).
+__device__ __forceinline__ void pair32_face(const float4* __restrict__ s4, int j, const Tgt32& F, float& p0,
+                                            float& p1, float& p2, float& p3) {
+  const float4 P = s4[j];  // x, y, z, area
+  const float4 Q = s4[2 * kNT + j];
+  const float dx = F.px - P.x, dy = F.py - P.y, dz = F.pz - P.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = rsqrtf(r2);
+  const float rinv2 = rinv * rinv;
+  const float fdd = Q.x * dx + Q.y * dy + Q.z * dz;
+  const float H1 = P.w * rinv;
+  const float H2 = fdd * H1 * rinv2;
+  p0 += Q.x * H1 + dx * H2;
+  p1 += Q.y * H1 + dy * H2;
+  p2 += Q.z * H1 + dz * H2;
+  p3 += fdd * (rinv2 * rinv) * P.w;
 }
 
 // ------------------------------------- FP32 on-surface pairs, all distances
@@ -744,13 +785,14 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   // FP64 below, FP32 above: (3 delta)^2 in the mixed mode; in the all-FP32 mode
   // only the r < 1e-14 limits of the reference stay in FP64
   const float cut2f = T.mixed == 2 ? 1e-28f : (float)(9.0 * T.DEL * T.DEL);
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;  // a3: the pressure of K_E2G_UP_AWAY
   unsigned long long creg = 0, cplain = 0, cfar = 0, cprox = 0;
-  constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY);
+  constexpr bool kFace = KIND == K_E2G_UP_AWAY;
+  constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY || kFace);
   // which path a target takes through a source tile
   constexpr bool kPerPairSplit = (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_SL_OFF || KIND == K_DL_OFF ||
                                    KIND == K_E2G_SL7 || KIND == K_E2G_P7);
-  const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY ||
+  const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY || kFace ||
                                ((KIND == K_SL_OFF || KIND == K_DL_OFF) && !S.near));
   // Each warp walks the item's segments on its own: its own source tiles in
   // shared memory, __syncwarp only, and an entry whose mask is zero for this
@@ -813,6 +855,21 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
             a1 += (double)p1;
             a2 += (double)p2;
           }
+        } else if (kFace && all32) {
+          for (int j0 = 0; j0 < cnt; j0 += 16) {
+            float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+            const int j1 = min(cnt, j0 + 16);
+            if (j1 - j0 == 16) {
+#pragma unroll 4
+              for (int j = j0; j < j0 + 16; j++) pair32_face(ws4, j, F, p0, p1, p2, p3);
+            } else {
+              for (int j = j0; j < j1; j++) pair32_face(ws4, j, F, p0, p1, p2, p3);
+            }
+            a0 += (double)p0;
+            a1 += (double)p1;
+            a2 += (double)p2;
+            a3 += (double)p3;
+          }
         } else if (all32) {
           for (int j0 = 0; j0 < cnt; j0 += 16) {
             float p0 = 0.f, p1 = 0.f, p2 = 0.f;
@@ -841,6 +898,15 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
             a1 += (double)p1;
             a2 += (double)p2;
           }
+        } else if (kFace) {
+          if (cnt == kNT) {
+#pragma unroll 4
+            for (int j = 0; j < kNT; j++) pair64_face(wsm, j, S, a0, a1, a2, a3);
+          } else {
+#pragma unroll 2
+            for (int j = 0; j < cnt; j++) pair64_face(wsm, j, S, a0, a1, a2, a3);
+          }
+          if (kCount) cfar += 2 * cnt;  // two sums' pairs
         } else {
           unsigned cr = 0;
           if (cnt == kNT) {  // a full tile: a compile-time trip count
@@ -906,10 +972,11 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
     }
   }
   // partial sums of this item
-  double* o = T.partial + ((size_t)it.slot * kTB + tid) * 3;
+  double* o = T.partial + ((size_t)it.slot * kTB + tid) * kPartComps;
   o[0] = a0;
   o[1] = a1;
   o[2] = a2;
+  o[3] = a3;
   // Work counters (pair kinds actually evaluated), one atomic per warp.
   if (kCount && T.counters) {
     for (int off = 16; off > 0; off >>= 1) {
@@ -1136,10 +1203,11 @@ __device__ __forceinline__ void run_item_on2(const EvalTask& T, const BlockRef& 
   }
 #pragma unroll
   for (int q = 0; q < 2; q++) {
-    double* o = T.partial + ((size_t)it.slot * kTB + warp * 64 + q * 32 + lane) * 3;
+    double* o = T.partial + ((size_t)it.slot * kTB + warp * 64 + q * 32 + lane) * kPartComps;
     o[0] = a[q][0];
     o[1] = a[q][1];
     o[2] = a[q][2];
+    o[3] = 0.0;
   }
 }
 
@@ -1234,7 +1302,8 @@ __global__ void __launch_bounds__(kTB, ON ? (FAM == F_DL ? 5 : 6) : ((FAM == F_S
     if (ON) run_item<K_DL_ON, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_DL_OFF, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else if (ON) {  // extend-to-grid: the plain box-face sums
-    if (kind == K_E2G_SL_AWAY) run_item<K_E2G_SL_AWAY, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    if (kind == K_E2G_UP_AWAY) run_item<K_E2G_UP_AWAY, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    else if (kind == K_E2G_SL_AWAY) run_item<K_E2G_SL_AWAY, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_E2G_P_AWAY, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else {  // extend-to-grid: the regularized band sums
     if (kind == K_E2G_SL7) run_item<K_E2G_SL7, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
@@ -1252,13 +1321,14 @@ __global__ void __launch_bounds__(kTB) reduce_kernel(const EvalTask* __restrict_
   const int k = blk * kTB + tid;
   if (k >= T.nt) return;
   const int t = T.tord[k];
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   const int s0 = T.item_start[blk], s1 = T.item_start[blk + 1];
   for (int s = s0; s < s1; s++) {
-    const double* p = T.partial + ((size_t)s * kTB + tid) * 3;
+    const double* p = T.partial + ((size_t)s * kTB + tid) * kPartComps;
     a0 += p[0];
     a1 += p[1];
     a2 += p[2];
+    a3 += p[3];
   }
   const double sc = T.scale;
   double* o = T.out;
@@ -1267,6 +1337,11 @@ __global__ void __launch_bounds__(kTB) reduce_kernel(const EvalTask* __restrict_
     o[3 * t] = a0 * sc;
     o[3 * t + 1] = a1 * sc;
     o[3 * t + 2] = a2 * sc;
+  } else if (kind == K_E2G_UP_AWAY) {
+    o[3 * t] = a0 * sc;
+    o[3 * t + 1] = a1 * sc;
+    o[3 * t + 2] = a2 * sc;
+    T.out2[t] = a3 * T.scale2;
   } else if (kind == K_DL_ON) {
     // DL[3i+k] = u[k] * EightPI6 + 0.5 * g0[k]   (2S/KITC.cpp:1693, 2S/stresslets.cpp:271-278)
     const double* g0 = T.tq + 3 * t;

@@ -409,7 +409,8 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
   // box-face sums), each part by decreasing cost
   auto on_kind = [&](const BlockRef& r) {
     const int k = tasks[r.task].kind;
-    return family == F_E2G ? (k == K_E2G_SL_AWAY || k == K_E2G_P_AWAY) : (k == K_SL_ON || k == K_DL_ON);
+    return family == F_E2G ? (k == K_E2G_SL_AWAY || k == K_E2G_P_AWAY || k == K_E2G_UP_AWAY)
+                           : (k == K_SL_ON || k == K_DL_ON);
   };
   std::stable_sort(items.begin(), items.end(),
                    [&](const std::pair<double, BlockRef>& a, const std::pair<double, BlockRef>& b) {
@@ -429,7 +430,7 @@ void Batch::finalize(cudaStream_t st, int num_sms) {
   d_segs.upload(segs, st);
   d_item_start.upload(starts, st);
   d_task_blocks.upload(tblocks, st);
-  d_partial.alloc((size_t)std::max(1, slot) * kTB * 3);
+  d_partial.alloc((size_t)std::max(1, slot) * kTB * kPartComps);
   for (size_t t = 0; t < tasks.size(); t++) {
     tasks[t].item_start = d_item_start.p + start_off[t];
     tasks[t].partial = d_partial.p;
