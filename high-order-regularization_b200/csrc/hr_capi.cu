@@ -135,6 +135,7 @@ Flops flops_of(int kind) {
     case K_E2G_SL_AWAY: return {31, 31, 31, 0};
     case K_E2G_P_AWAY: return {18, 18, 18, 0};
     case K_E2G_UP_AWAY: return {24.5, 24.5, 24.5, 0};  // per counted pair: each fused pair counts twice
+    case K_E2G_UP7: return {61.5, 42, 42, 0};
     case K_E2G_SL7: return {59, 37, 37, 0};
     default: return {64, 47, 47, 0};
   }

@@ -3,7 +3,9 @@
 //   1. pressure and velocity boundary integrals at the six box faces with the
 //      plain kernels and at the BAND1 grid points outside or on the surface
 //      with the 7th-order regularized kernels and subtraction (one batched
-//      launch of four sums, E2G/main.cpp:1049-1406);
+//      launch of the four sums, E2G/main.cpp:1049-1406, as two passes: velocity
+//      and pressure at the same targets share each pair's distance and
+//      smoothing factors);
 //   2. p = 0 and u = (1, 0, 0) elsewhere, then the four Poisson extensions:
 //      p first (variable 0), then u_x, u_y, u_z with the extended p
 //      (E2G/main.cpp:195-200, 403-424).
@@ -269,15 +271,17 @@ static void e2g_batch(hr_e2g& E, int prec, Ctx& C) {
   EvalTask a = make_task(K_E2G_UP_AWAY, delta, sl_scale, E.tree, E.Lf, E.tf, E.uf.p);
   a.out2 = E.pf.p;
   a.scale2 = p_scale;
-  EvalTask c = make_task(K_E2G_P7, delta, -p_scale, E.tree, E.Lb, E.tb, E.pb.p);
-  EvalTask d = make_task(K_E2G_SL7, delta, sl_scale, E.tree, E.Lb, E.tb, E.ub.p);
-  for (EvalTask* t : {&a, &c, &d}) {
+  // and the two band sums likewise
+  EvalTask c = make_task(K_E2G_UP7, delta, sl_scale, E.tree, E.Lb, E.tb, E.ub.p);
+  c.out2 = E.pb.p;
+  c.scale2 = -p_scale;
+  for (EvalTask* t : {&a, &c}) {
     t->mixed = prec;
     t->jump_mode = 1;
   }
-  B.tasks = {a, c, d};
-  B.lists = {&E.Lf.host, &E.Lb.host, &E.Lb.host};
-  B.trees = {&E.tree.host, &E.tree.host, &E.tree.host};
+  B.tasks = {a, c};
+  B.lists = {&E.Lf.host, &E.Lb.host};
+  B.trees = {&E.tree.host, &E.tree.host};
   B.finalize(C.stream, C.num_sms);
 }
 

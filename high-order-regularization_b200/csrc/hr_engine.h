@@ -18,6 +18,7 @@ enum Kind : int {
   K_E2G_SL7 = 6,      // stokes_SL_7ord                    E2G/stokes.cpp:53-97
   K_E2G_P7 = 7,       // stokes_pressure_7ord              E2G/stokes.cpp:134-203
   K_E2G_UP_AWAY = 8,  // stokes_SL_away + stokes_pressure_away at the same targets, one pass
+  K_E2G_UP7 = 9,      // stokes_SL_7ord + stokes_pressure_7ord at the same targets, one pass
 };
 
 constexpr int kTB = 128;  // targets per target block = threads per CTA

@@ -138,7 +138,7 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
   for (int k = 0; k < 3; k++) S.x0[k] = S.n0[k] = S.g0[k] = S.n0xf0[k] = 0.0;
   S.c.c1 = S.c.c2 = S.c.c3 = 0.0;
   // regularized-kernel kinds: on-surface sums and the E2G band sums
-  S.near = (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_E2G_SL7 || KIND == K_E2G_P7) ? 1 : 0;
+  S.near = (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_E2G_SL7 || KIND == K_E2G_P7 || KIND == K_E2G_UP7) ? 1 : 0;
   if (valid) {
     S.px = T.txyz[3 * t];
     S.py = T.txyz[3 * t + 1];
@@ -165,7 +165,7 @@ __device__ __forceinline__ void load_target(const EvalTask& T, int t, bool valid
         S.g0[k] = T.tg0[3 * t + k];
       }
       if (S.near) S.c = reg_coeff(S.b / T.DEL);
-    } else if (KIND == K_E2G_P7) {
+    } else if (KIND == K_E2G_P7 || KIND == K_E2G_UP7) {
       S.b = T.tb[t];
       double f0[3], n0[3];
       for (int k = 0; k < 3; k++) {
@@ -374,6 +374,52 @@ __device__ __forceinline__ void pair64_face(const double* __restrict__ sm, int j
   a3 += (fdd * (rinv * rinv * rinv)) * Aj;
 }
 
+// The band sums of one target in one pass (K_E2G_UP7): stokes_SL_7ord and
+// stokes_pressure_7ord (E2G/stokes.cpp:53-97, 134-203) share the offset, the
+// distance and the regularized factors' erf and exp (sl_lapl_7ord); each
+// keeps the expressions of its own kind above; a3 collects the pressure.
+// Returns true if the smoothed branch was taken.
+__device__ __forceinline__ bool pair64_band(const double* __restrict__ sm, int j, const Tgt& S, const Reg& g,
+                                            double& a0, double& a1, double& a2, double& a3) {
+  const double2* s2v = reinterpret_cast<const double2*>(sm) + 5 * j;
+  const double2 v0 = s2v[0], v1 = s2v[1], v2 = s2v[2], v3 = s2v[3], v4 = s2v[4];
+  const double Xj = v0.x, Yj = v0.y, Zj = v1.x, Aj = v1.y;
+  const double NXj = v2.x, NYj = v2.y, NZj = v3.x, QXj = v3.y, QYj = v4.x, QZj = v4.y;
+  const double dx = S.px - Xj, dy = S.py - Yj, dz = S.pz - Zj;
+  const double r2 = dx * dx + dy * dy + dz * dz;
+  const double rinv = rsqrt(r2);
+  double H1, H2, H2p;
+  const bool reg = sl_lapl_7ord(r2, rinv, g, S.c, H1, H2, H2p);
+  {
+    const double area = Aj;
+    const double fx = QXj - S.f0n0 * NXj;
+    const double fy = QYj - S.f0n0 * NYj;
+    const double fz = QZj - S.f0n0 * NZj;
+    const double fdd = fx * dx + fy * dy + fz * dz;
+    H1 *= area;
+    H2 *= area * fdd;
+    a0 += fx * H1 + dx * H2;
+    a1 += fy * H1 + dy * H2;
+    a2 += fz * H1 + dz * H2;
+  }
+  {
+    const double n0 = NXj, n1 = NYj, n2 = NZj;
+    const double f0 = QXj, f1 = QYj, f2 = QZj;
+    const double f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
+    const double ncf0 = (n1 * f2 - n2 * f1) - S.n0xf0[0];
+    const double ncf1 = (n2 * f0 - n0 * f2) - S.n0xf0[1];
+    const double ncf2 = (n0 * f1 - n1 * f0) - S.n0xf0[2];
+    const double n_dot_dx = n0 * dx + n1 * dy + n2 * dz;
+    const double ncd0 = n1 * dz - n2 * dy;
+    const double ncd1 = n2 * dx - n0 * dz;
+    const double ncd2 = n0 * dy - n1 * dx;
+    const double normal = -(f_dot_n - S.f0n0) * n_dot_dx;
+    const double tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
+    a3 += (normal + tangential) * H2p * Aj;
+  }
+  return reg;
+}
+
 // ------------------------------------------------------- FP32 plain pairs
 // The singular kernel of each kind (the r/delta > 8 branch of the reference),
 // from FP32 centre-relative coordinates.
@@ -453,6 +499,48 @@ __device__ __forceinline__ void pair32_face(const float4* __restrict__ s4, int j
   p1 += Q.y * H1 + dy * H2;
   p2 += Q.z * H1 + dz * H2;
   p3 += fdd * (rinv2 * rinv) * P.w;
+}
+
+// The band sums in FP32 in one pass, for pairs with r > 3 delta (as pair32r
+// of K_E2G_SL7 and of K_E2G_P7, sharing sl_lapl_7ord_f).
+__device__ __forceinline__ bool pair32r_band(const float4* __restrict__ s4, int j, const Tgt32& F, const RegF& gf,
+                                             float& p0, float& p1, float& p2, float& p3) {
+  const float4 P = s4[j];  // x, y, z, area
+  const float4 N = s4[kNT + j];
+  const float4 Q = s4[2 * kNT + j];
+  const float dx = F.px - P.x, dy = F.py - P.y, dz = F.pz - P.z;
+  const float r2 = dx * dx + dy * dy + dz * dz;
+  const float rinv = rsqrtf(r2);
+  const bool reg = r2 <= gf.d64;
+  float H1, H2, H2p;
+  sl_lapl_7ord_f(r2, rinv, gf, F.c, H1, H2, H2p);
+  {
+    const float fx = Q.x - F.f0n0 * N.x;
+    const float fy = Q.y - F.f0n0 * N.y;
+    const float fz = Q.z - F.f0n0 * N.z;
+    const float fdd = fx * dx + fy * dy + fz * dz;
+    H1 *= P.w;
+    H2 *= P.w * fdd;
+    p0 += fx * H1 + dx * H2;
+    p1 += fy * H1 + dy * H2;
+    p2 += fz * H1 + dz * H2;
+  }
+  {
+    const float n0 = N.x, n1 = N.y, n2 = N.z;
+    const float f0 = Q.x, f1 = Q.y, f2 = Q.z;
+    const float f_dot_n = f0 * n0 + f1 * n1 + f2 * n2;
+    const float ncf0 = (n1 * f2 - n2 * f1) - F.n0xf0[0];
+    const float ncf1 = (n2 * f0 - n0 * f2) - F.n0xf0[1];
+    const float ncf2 = (n0 * f1 - n1 * f0) - F.n0xf0[2];
+    const float n_dot_dx = n0 * dx + n1 * dy + n2 * dz;
+    const float ncd0 = n1 * dz - n2 * dy;
+    const float ncd1 = n2 * dx - n0 * dz;
+    const float ncd2 = n0 * dy - n1 * dx;
+    const float normal = -(f_dot_n - F.f0n0) * n_dot_dx;
+    const float tangential = -(ncf0 * ncd0 + ncf1 * ncd1 + ncf2 * ncd2);
+    p3 += (normal + tangential) * H2p * P.w;
+  }
+  return reg;
 }
 
 // ------------------------------------- FP32 on-surface pairs, all distances
@@ -791,7 +879,8 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
   constexpr bool kSrcNrm = !(KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY || kFace);
   // which path a target takes through a source tile
   constexpr bool kPerPairSplit = (KIND == K_SL_ON || KIND == K_DL_ON || KIND == K_SL_OFF || KIND == K_DL_OFF ||
-                                   KIND == K_E2G_SL7 || KIND == K_E2G_P7);
+                                   KIND == K_E2G_SL7 || KIND == K_E2G_P7 || KIND == K_E2G_UP7);
+  constexpr bool kBand = KIND == K_E2G_UP7;
   const bool all32 = MIXED && (KIND == K_E2G_SL_AWAY || KIND == K_E2G_P_AWAY || kFace ||
                                ((KIND == K_SL_OFF || KIND == K_DL_OFF) && !S.near));
   // Each warp walks the item's segments on its own: its own source tiles in
@@ -888,15 +977,34 @@ __device__ __forceinline__ void run_item(const EvalTask& T, const BlockRef& it,
           for (int j0 = 0; j0 < cnt; j0 += 16) {
             float p0 = 0.f, p1 = 0.f, p2 = 0.f;
             const int j1 = min(cnt, j0 + 16);
+            float p3 = 0.f;
             for (int j = j0; j < j1; j++) {
               const float4 Pj = ws4[j];
               const float dx = F.px - Pj.x, dy = F.py - Pj.y, dz = F.pz - Pj.z;
-              if (dx * dx + dy * dy + dz * dz > cut2f) pair32r<KIND>(ws4, j, F, gf, p0, p1, p2);
-              else pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
+              if (kBand) {
+                if (dx * dx + dy * dy + dz * dz > cut2f) pair32r_band(ws4, j, F, gf, p0, p1, p2, p3);
+                else pair64_band(wsm, j, S, g, a0, a1, a2, a3);
+              } else {
+                if (dx * dx + dy * dy + dz * dz > cut2f) pair32r<KIND>(ws4, j, F, gf, p0, p1, p2);
+                else pair64<KIND>(wsm, j, S, g, stab, a0, a1, a2);
+              }
             }
             a0 += (double)p0;
             a1 += (double)p1;
             a2 += (double)p2;
+            a3 += (double)p3;
+          }
+        } else if (kBand) {
+          unsigned cr = 0;
+          if (cnt == kNT) {
+#pragma unroll 2
+            for (int j = 0; j < kNT; j++) cr += pair64_band(wsm, j, S, g, a0, a1, a2, a3);
+          } else {
+            for (int j = 0; j < cnt; j++) cr += pair64_band(wsm, j, S, g, a0, a1, a2, a3);
+          }
+          if (kCount) {  // two sums' pairs
+            creg += 2 * cr;
+            cplain += 2 * (cnt - cr);
           }
         } else if (kFace) {
           if (cnt == kNT) {
@@ -1306,7 +1414,8 @@ __global__ void __launch_bounds__(kTB, ON ? (FAM == F_DL ? 5 : 6) : ((FAM == F_S
     else if (kind == K_E2G_SL_AWAY) run_item<K_E2G_SL_AWAY, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_E2G_P_AWAY, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   } else {  // extend-to-grid: the regularized band sums
-    if (kind == K_E2G_SL7) run_item<K_E2G_SL7, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    if (kind == K_E2G_UP7) run_item<K_E2G_UP7, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
+    else if (kind == K_E2G_SL7) run_item<K_E2G_SL7, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
     else run_item<K_E2G_P7, MIXED, COUNT>(sT, it, segs, sm, sf, cheb, chebf, stab, stab32);
   }
 }
@@ -1342,6 +1451,18 @@ __global__ void __launch_bounds__(kTB) reduce_kernel(const EvalTask* __restrict_
     o[3 * t + 1] = a1 * sc;
     o[3 * t + 2] = a2 * sc;
     T.out2[t] = a3 * T.scale2;
+  } else if (kind == K_E2G_UP7) {
+    o[3 * t] = a0 * sc;
+    o[3 * t + 1] = a1 * sc;
+    o[3 * t + 2] = a2 * sc;
+    // p *= -denom_FourPI (scale2); inside: p -= f0.n0 (E2G/stokes.cpp:196-200)
+    double p = a3 * T.scale2;
+    if (T.tb[t] < -1.e-12) {
+      const double* f0 = T.tf0 + 3 * t;
+      const double* n0 = T.tn0 + 3 * t;
+      p -= f0[0] * n0[0] + f0[1] * n0[1] + f0[2] * n0[2];
+    }
+    T.out2[t] = p;
   } else if (kind == K_DL_ON) {
     // DL[3i+k] = u[k] * EightPI6 + 0.5 * g0[k]   (2S/KITC.cpp:1693, 2S/stresslets.cpp:271-278)
     const double* g0 = T.tq + 3 * t;

@@ -209,6 +209,42 @@ __device__ __forceinline__ bool lapl_dl_7ord(double r2, double rinv, const Reg& 
   return true;
 }
 
+// sl_7ord and lapl_dl_7ord of one pair together: s1, s2 as sl_7ord, s2p as
+// lapl_dl_7ord (its own association of the last polynomial term), sharing
+// the powers of r/delta, erf and exp.
+__device__ __forceinline__ bool sl_lapl_7ord(double r2, double rinv, const Reg& g, const Coef& c, double& s1,
+                                             double& s2, double& s2p) {
+  const double rp = d_rootpi();
+  if (r2 < g.r0sq) {
+    s1 = 32.0 / 5.0 / rp / g.d;
+    s2 = 256.0 / 15.0 / rp / (g.d * g.d * g.d);
+    s2p = s2;
+    return false;
+  }
+  double rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s1 = rinv;
+    s2 = rinv3;
+    s2p = rinv3;
+    return false;
+  }
+  double rd = r2 * rinv * g.inv_d;
+  double rd2 = rd * rd;
+  double rd4 = rd2 * rd2;
+  double rd6 = rd4 * rd2;
+  double errfn = erf(rd);
+  double r_expfn = rd * exp(-rd2);
+  double poly1 = c.c1 - 2.0 * (c.c2 + c.c3) * rd2 + 4.0 * c.c3 * rd4;
+  double poly2 = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
+                 4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd6;
+  double poly2p = -2.0 / rp + 2.0 * (c.c1 + 2.0 * (c.c2 + c.c3)) * rd2 -
+                  4.0 * (c.c2 + 5.0 * c.c3) * rd4 + 8.0 * c.c3 * rd4 * rd2;
+  s1 = (errfn + poly1 * r_expfn) * rinv;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  s2p = (errfn + poly2p * r_expfn) * rinv3;
+  return true;
+}
+
 }  // namespace hr
 
 // ------------------------------------------------------------------ FP32 forms
@@ -296,6 +332,28 @@ __device__ __forceinline__ void dl_7ord_onsurf_f(float r2, float rinv, const Reg
   const float errfn = erff(rd), r_expfn = 2.0f / kRootPiF * rd * expf(-rd2);
   const float poly3 = -1.0f - 2.0f / 3.0f * rd2 + 52.0f / 45.0f * rd4 - 8.0f / 45.0f * rd6;
   s3 = (errfn + poly3 * r_expfn) * rinv5;
+}
+
+// sl_7ord_f and lapl_dl_7ord_f of one pair together (as sl_lapl_7ord).
+__device__ __forceinline__ void sl_lapl_7ord_f(float r2, float rinv, const RegF& g, const CoefF& c, float& s1,
+                                               float& s2, float& s2p) {
+  const float rinv3 = rinv * rinv * rinv;
+  if (r2 > g.d64) {
+    s1 = rinv;
+    s2 = rinv3;
+    s2p = rinv3;
+    return;
+  }
+  const float rd = r2 * rinv * g.inv_d, rd2 = rd * rd, rd4 = rd2 * rd2, rd6 = rd4 * rd2;
+  const float errfn = erff(rd), r_expfn = rd * expf(-rd2);
+  const float poly1 = c.c1 - 2.0f * (c.c2 + c.c3) * rd2 + 4.0f * c.c3 * rd4;
+  const float poly2 = -2.0f / kRootPiF + 2.0f * (c.c1 + 2.0f * (c.c2 + c.c3)) * rd2 -
+                      4.0f * (c.c2 + 5.0f * c.c3) * rd4 + 8.0f * c.c3 * rd6;
+  const float poly2p = -2.0f / kRootPiF + 2.0f * (c.c1 + 2.0f * (c.c2 + c.c3)) * rd2 -
+                       4.0f * (c.c2 + 5.0f * c.c3) * rd4 + 8.0f * c.c3 * rd4 * rd2;
+  s1 = (errfn + poly1 * r_expfn) * rinv;
+  s2 = (errfn + poly2 * r_expfn) * rinv3;
+  s2p = (errfn + poly2p * r_expfn) * rinv3;
 }
 
 __device__ __forceinline__ void lapl_dl_7ord_f(float r2, float rinv, const RegF& g, const CoefF& c, float& s2) {
