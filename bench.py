@@ -229,7 +229,7 @@ def run_reference(args, rank, world):
         return
     R = Ref2S(P, N0).setup(H_INV)
     # pair count of one operator application (target-source plus target-proxy
-    # evaluations of its four treecode sums), from the checker's statistics on
+    # evaluations of its four treecode sums), from the oracle's statistics on
     # the reference's own geometry; the count does not depend on the density
     from oracle import Oracle
 

@@ -11,7 +11,7 @@ namespace hr {
 
 namespace {
 
-// Freed blocks the pool keeps mapped before it returns memory to the driver.
+// Freed blocks the pool keeps mapped before it returns memory to the CUDA driver.
 constexpr uint64_t kPoolKeepBytes = 8ull << 30;
 constexpr int kMaxDevices = 64;
 

@@ -1,9 +1,9 @@
-"""Build recipe for the checker (oracle) libraries.
+"""Build recipe for the oracle libraries.
 
 Two things are built here, both test infrastructure only:
 
 1. ``oracle/liboracle.so`` from ``oracle/highreg_oracle.c``: the plain-C
-   restatement of the reference's hot-path algorithm (the checker that the GPU
+   restatement of the reference's hot-path algorithm (the oracle that the GPU
    parity tests compare against). Built with ``gcc -O2`` and no ``-march`` so
    that, like the reference built the same way, no fused multiply-adds are
    emitted and the scalar arithmetic follows the reference's operation order.
@@ -18,7 +18,7 @@ Two things are built here, both test infrastructure only:
    here) is replaced by the test-only header ``fftw_standin/fftw3.h``.
 
 ``oracle/_ref`` is git-ignored but travels with the working tree, so the
-checker can use it wherever it was built; the reference tree itself is only
+oracle can use it wherever it was built; the reference tree itself is only
 read at build time.
 """
 from __future__ import annotations
@@ -67,7 +67,7 @@ def _newer(target, sources):
     return all(os.path.getmtime(s) <= t for s in sources if os.path.exists(s))
 
 
-def build_checker(force: bool = False) -> str:
+def build_oracle_lib(force: bool = False) -> str:
     src = os.path.join(HERE, "highreg_oracle.c")
     out = os.path.join(HERE, "liboracle.so")
     if force or not _newer(out, [src, os.path.join(HERE, "highreg_oracle.h")]):
@@ -186,7 +186,7 @@ def build_relinked_e2g(force: bool = False, root: str | None = None):
 
 
 def build_all(force: bool = False) -> None:
-    build_checker(force)
+    build_oracle_lib(force)
     build_reference(force)
 
 

@@ -1,7 +1,7 @@
 /*
  * highreg_oracle.c — plain-C restatement of the reference's hot path.
  *
- * TEST INFRASTRUCTURE ONLY. This file is the checker: tests/, the smoke test
+ * TEST INFRASTRUCTURE ONLY. This file is the oracle: tests/, the smoke test
  * and the CPU-baseline leg of bench.py call it to produce the expected answer.
  * The product (high-order-regularization_b200/) never links, loads or calls it.
  *

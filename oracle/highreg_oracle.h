@@ -1,6 +1,6 @@
 /*
  * highreg_oracle.h — CPU restatement of the reference's hot path, used ONLY as
- * the checker by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * the oracle by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
  * leg. It is never linked into the product library.
  *
  * Conventions (same as the reference): vector fields and points are

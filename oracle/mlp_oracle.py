@@ -9,7 +9,7 @@ beta2 0.999, eps 1e-8). Parameter layout: W1[12][64] b1[64] W2[64][64] b2[64]
 W3[64][64] b3[64] W4[64][3] b4[3], W[i][j] from input i to output j.
 
 It is pinned by a finite-difference check of its own gradient (tests), and
-it is the checker for the CUDA forward, gradient and Adam kernels. Nothing in
+it is the oracle for the CUDA forward, gradient and Adam kernels. Nothing in
 the product imports it.
 """
 import numpy as np

@@ -1,4 +1,4 @@
-"""ctypes front end of the checker (test infrastructure only).
+"""ctypes front end of the oracle (test infrastructure only).
 
 ``Oracle`` wraps ``oracle/liboracle.so`` (the C restatement of the reference's
 hot path); ``Ref2S`` and ``RefE2G`` wrap the reference programs compiled from
@@ -51,7 +51,7 @@ class Oracle:
         if not os.path.exists(path):
             import build_oracle  # noqa: local module
 
-            build_oracle.build_checker()
+            build_oracle.build_oracle_lib()
         self.lib = ctypes.CDLL(path)
         L = self.lib
         L.or_dl_7ord_onsurf.restype = ctypes.c_double
@@ -330,7 +330,7 @@ class Ref2S:
         return x, r[:k]
 
     def load(self, geo: dict, g=None):
-        """Loads a scene in the checker's dict layout (see Oracle.scene) into
+        """Loads a scene in the oracle's dict layout (see Oracle.scene) into
         the reference program instead of its own set-up; g (optional, per
         surface) is the stresslet density."""
         for s in (0, 1):
@@ -358,7 +358,7 @@ class Ref2S:
         return out, g0
 
     def geometry(self):
-        """Scene geometry in the checker's dict layout (see Oracle.scene)."""
+        """Scene geometry in the oracle's dict layout (see Oracle.scene)."""
         ctrs = [(0.0, 0.0, -0.5 - 1.0 / 4096.0), (0.0, 0.0, 0.5)]
         geo = dict(h=self.h, DEL=self.DEL)
         for s in (0, 1):

@@ -1,7 +1,7 @@
 // Test-only wrapper: exposes the UNMODIFIED reference two-surface program
 // (highreg_stokes_2surf/*.cpp, compiled from where it lies by
 // oracle/build_oracle.py) through flat extern "C" entry points, so that the
-// checker can drive the reference's own functions on identical inputs.
+// oracle can drive the reference's own functions on identical inputs.
 //
 // It holds one "scene" exactly as 2S/main.cpp:67-130 and
 // 2S/main.cpp:147-177 build it (two spheroids, on-surface targets, nearest

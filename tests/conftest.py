@@ -22,7 +22,7 @@ def oracle():
     import build_oracle
     from oracle import Oracle
 
-    build_oracle.build_checker()
+    build_oracle.build_oracle_lib()
     return Oracle()
 
 

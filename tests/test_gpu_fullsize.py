@@ -1,5 +1,5 @@
 """The benchmark's full sizes, checked through size-independent properties
-(the checker cannot run them in seconds):
+(the oracle cannot run them in seconds):
 
 * extend-to-grid at N = 384 (h = 3/384): the error against the exact
   translating-spheroid solution falls by two orders from N = 96 (the

@@ -30,7 +30,7 @@ def test_reference_driver_on_gpu(tmp_path, oracle):
     ref_hist = [6.19915e-02, 7.14192e-03, 8.84480e-04, 1.22093e-04, 2.40454e-05, 3.99025e-06, 6.06091e-07,
                 1.00332e-07, 2.29270e-08, 6.67164e-09, 1.58622e-09, 3.25818e-10, 7.82140e-11]
     assert np.allclose(hist, ref_hist, rtol=1e-4)
-    # the written solution against the checker's solve of the same system
+    # the written solution against the oracle's solve of the same system
     import highreg
 
     G = highreg.Geometry2S(32).scene

@@ -1,5 +1,5 @@
 """GPU parity of the two-surface operator, right-hand side and GMRES solve
-(2S/main.cpp:140-677) against the reference's golden outputs and the checker."""
+(2S/main.cpp:140-677) against the reference's golden outputs and the oracle."""
 import numpy as np
 import pytest
 
@@ -52,7 +52,7 @@ def test_solve_matches_reference(plan16, g2s):
 
 def test_solution_satisfies_system_under_oracle_operator(plan16, g2s, oracle):
     """Size-independent property: the GPU solution x satisfies A x = b with the
-    checker's own operator, to the solve tolerance."""
+    oracle's own operator, to the solve tolerance."""
     sc = oracle.scene(g2s, tree=True, P=int(g2s["P"]), N0=int(g2s["N0"]))
     b = oracle.rhs_2s(sc, g2s["f0"], g2s["f1"])
     x, rep = plan16.solve(b, restart=50, tol=1e-10)

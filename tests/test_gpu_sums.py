@@ -1,5 +1,5 @@
 """GPU parity of the boundary sums against the reference's golden outputs and
-the checker, through the C ABI.
+the oracle, through the C ABI.
 
 Tolerance (FP64 path): max |gpu - ref| <= 1e-12 * max |ref|. The GPU sums
 contract multiply-adds into FMAs and add the same terms in a different order

@@ -1,4 +1,4 @@
-"""Pins the checker (oracle/highreg_oracle.c) to the reference's own outputs.
+"""Pins the oracle (oracle/highreg_oracle.c) to the reference's own outputs.
 
 The golden fixtures were produced by the unmodified reference
 (tests/golden/make_golden.py); the C restatement must reproduce them bit for
