@@ -197,7 +197,7 @@ void lu4_solve(const double A[4][4], const int p[4], const double b[4], double x
 }
 
 // find_Nearest: E2G/surface.cpp:204-295
-int find_nearest(const double* pt, const double* start, double* x0, double* n0) {
+int find_nearest(const double* pt, const double* start, double* x0, double* n0, double* lam_out = nullptr) {
   double x[3] = {start[0], start[1], start[2]};
   double F[4] = {phi(x), x[0] - pt[0], x[1] - pt[1], x[2] - pt[2]};
   double Fn = F[0] * F[0] + F[1] * F[1] + F[2] * F[2] + F[3] * F[3];
@@ -224,6 +224,7 @@ int find_nearest(const double* pt, const double* start, double* x0, double* n0) 
     n = n + 1;
   }
   if (n > 100) return -1;
+  if (lam_out) *lam_out = lam;
   for (int k = 0; k < 3; k++) x0[k] = x[k];
   double a = dphi(0, x), b = dphi(1, x), c = dphi(2, x);
   double nn = sqrt(a * a + b * b + c * c);
@@ -412,12 +413,24 @@ void build(Scene& S, int N, double band1, double band2) {
     Tag t;
     t.g = g;
     t.q = claim[g].load(std::memory_order_relaxed);
+    double lam = 0.0;
+    bool converged = false;
     auto attempt = [&](int q2) {
-      if (find_nearest(pt, &S.xq[3 * q2], t.x0, t.n0) != 0) return false;
+      converged = false;
+      if (find_nearest(pt, &S.xq[3 * q2], t.x0, t.n0, &lam) != 0) return false;
+      converged = true;
       t.b = (pt[0] - t.x0[0]) * t.n0[0] + (pt[1] - t.x0[1]) * t.n0[1] + (pt[2] - t.x0[2]) * t.n0[2];
       return fabs(t.b) <= (band1 * h + tol);
     };
     bool tagged = attempt(t.q);
+    // At a converged point pt - x0 = lam grad phi(x0); on this ellipsoid the
+    // nearest surface point is the one critical point with 2 lam > -min a_i^2
+    // (x0_i - c_i = a_i^2 (pt_i - c_i) / (a_i^2 + 2 lam), the root of a
+    // decreasing function there), and |b| = |pt - x0| is then the distance.
+    // When it already exceeds the band, every start ends at a point at least
+    // as far, so the later attempts below would all fail.
+    const bool nearest = converged && 2.0 * lam > -0.25 * (1.0 - 1e-6);  // min a_i^2 = 0.25
+    if (!tagged && nearest && fabs(t.b) > band1 * h + tol + 1e-10 * h) continue;
     if (!tagged) {
       // The reference leaves the point untagged and tries again from every
       // later quadrature point whose neighbourhood contains it
