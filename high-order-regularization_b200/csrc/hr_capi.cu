@@ -979,8 +979,9 @@ extern "C" int hr_plan2s_create(hr_ctx* ctx, const hr_scene2s* sc, const hr_eval
       upload_targets(P->tg[t], T.n, sc->surf[t].xyz, T.b, T.x0, T.n0, sc->f0[t], sc->surf[t].nrml,
                      near, st);
       std::vector<uint8_t> all(T.n, 1);
-      P->Lon[t].build(P->tree[t].host, T.n, sc->surf[t].xyz, all.data(), st);
-      P->Loff[t].build(P->tree[1 - t].host, T.n, sc->surf[t].xyz, near.data(), st);
+      const std::vector<int> mo = morton_order(T.n, sc->surf[t].xyz);  // shared by both lists
+      P->Lon[t].build(P->tree[t].host, T.n, sc->surf[t].xyz, all.data(), st, &mo);
+      P->Loff[t].build(P->tree[1 - t].host, T.n, sc->surf[t].xyz, near.data(), st, &mo);
       check_i123(T.n, T.nrst, T.i123);
       P->hnrst[t].assign(T.nrst, T.nrst + T.n);
       P->hi123[t].assign(T.i123, T.i123 + 3 * (size_t)T.n);
@@ -1033,8 +1034,9 @@ extern "C" int hr_plan2s_set_inner_tree(hr_plan2s* plan, int P, int N0, double t
     for (int s = 0; s < 2; s++) in->tree[s].build(Q.surf_host[s], P, N0, theta, false, st);
     for (int t = 0; t < 2; t++) {
       std::vector<uint8_t> all(Q.nq[t], 1);
-      in->Lon[t].build(in->tree[t].host, Q.nq[t], Q.surf_host[t].xyz, all.data(), st);
-      in->Loff[t].build(in->tree[1 - t].host, Q.nq[t], Q.surf_host[t].xyz, Q.near_host[t].data(), st);
+      const std::vector<int> mo = morton_order(Q.nq[t], Q.surf_host[t].xyz);
+      in->Lon[t].build(in->tree[t].host, Q.nq[t], Q.surf_host[t].xyz, all.data(), st, &mo);
+      in->Loff[t].build(in->tree[1 - t].host, Q.nq[t], Q.surf_host[t].xyz, Q.near_host[t].data(), st, &mo);
     }
     dl_batches(Q, in->tree, in->Lon, in->Loff, in->dl, 1, 3, false, Q.C->stream);
     // accuracy of the inner operator (mixed precision) against the plan's FP64

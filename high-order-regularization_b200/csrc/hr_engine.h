@@ -70,7 +70,9 @@ struct Lists {
 // (2S/KITC.cpp:1066-1386): far if node.MAC < |x - node centre|^2, else a
 // direct sum if (m1 - m0) < N0, else recurse into the children in order.
 // near[t] (may be null) marks targets that take the regularized branch.
-Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near);
+// morton (optional): the targets' morton_order, when the caller has it already.
+Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near,
+                  const std::vector<int>* morton = nullptr);
 
 // Density-interpolation stencils (2S/main.cpp:682-1046): for every target with
 // nrst != 0, the 6x6 source indices (reference order; unset slots read 0) and

@@ -234,8 +234,8 @@ void DevTree::set_density(Ctx& C, const double* q3_dev, bool dl, bool moments, b
 }
 
 void DevLists::build(const Tree& T, int nt, const double* txyz, const uint8_t* near,
-                     cudaStream_t st) {
-  host = build_lists(T, nt, txyz, near);
+                     cudaStream_t st, const std::vector<int>* morton) {
+  host = build_lists(T, nt, txyz, near, morton);
   tord.upload(host.tord, st);
   blk_start.upload(host.blk_start, st);
   entries.upload(host.entries, st);

@@ -150,7 +150,8 @@ struct DevLists {
   Lists host;
   DBuf<int> tord, blk_start;
   DBuf<Entry> entries;
-  void build(const Tree& T, int nt, const double* txyz, const uint8_t* near, cudaStream_t st);
+  void build(const Tree& T, int nt, const double* txyz, const uint8_t* near, cudaStream_t st,
+             const std::vector<int>* morton = nullptr);
 };
 
 struct DevStencils {

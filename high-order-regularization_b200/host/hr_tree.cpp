@@ -225,9 +225,10 @@ std::vector<int> morton_order(int n, const double* xyz) {
   return ord;
 }
 
-Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near) {
+Lists build_lists(const Tree& T, int nt, const double* txyz, const uint8_t* near,
+                  const std::vector<int>* morton) {
   Lists L;
-  L.tord = morton_order(nt, txyz);
+  L.tord = morton ? *morton : morton_order(nt, txyz);
   const int nb = (nt + kTB - 1) / kTB;
   const int nn = T.nnodes();
   const int P1 = T.P + 1;
